@@ -1,0 +1,187 @@
+/*
+ * g6b200.h -- C ABI of the B200 GRAPE-6 force engine (libg6b200.so).
+ *
+ * The first block is the GRAPE-6 host-library ABI exactly as Starlab's
+ * include/grape6.h:16-104 declares it and src/node/dyn/hdyn/evolve/
+ * hdyn_grape6.C calls it: Fortran-style trailing underscores, every scalar by
+ * pointer, `vec` arrays as double[][3] (include/starlab_vector.h: a vec is
+ * three contiguous doubles).  Linking kira/hsys_stats/hscale against this
+ * library ahead of the reference's null stubs
+ * (src/node/dyn/hdyn/stubs/grape6_stubs.c) makes g6_npipes_() > 0, so kira
+ * selects its GRAPE-6 code path (kira_config.C:62) unchanged.
+ *
+ * Semantics shared by all entry points:
+ *   - cluster_id selects an independent engine instance (device-resident
+ *     j-memory); kira always uses 0.  Instances open lazily.
+ *   - int returns: 0 = OK.  g6calc_lasthalf*_ nonzero = engine error (kira
+ *     then resets, reopens, reloads j and retries: hdyn_grape6.C:892-899).
+ *   - j-particle updates are staged on the host and reach the device at the
+ *     next g6calc_firsthalf_ / g6_flush_jp_buffer_.
+ *   - g6calc_firsthalf_ starts the computation asynchronously; the matching
+ *     g6calc_lasthalf*_ waits and writes the results.  Calls alternate.
+ *   - The engine computes, for each i, the sum over j in [0, nj), j != the
+ *     i's index, of the softened Newtonian pair terms (hdyn_ev.C:2019-2036):
+ *     acc, full jerk, pot (< 0), plus the nearest neighbour address (r^2
+ *     without softening, first address on ties) and, for h2[i] > 0, the
+ *     neighbour list {j : |x_j - x_i|^2 < h2[i]}.
+ *   - Precision mode per instance (g6b200_set_precision, or the environment
+ *     variable G6B200_PRECISION=fp64|mixed read at open):
+ *       G6B200_FP64  : FP64 prediction, differences, pair math, accumulation.
+ *       G6B200_MIXED : FP64 prediction; positions as 47-bit fixed point held
+ *                      in two FP32 words so x_j - x_i is exact before its one
+ *                      rounding to FP32; FP32 pair math with a Newton-refined
+ *                      rsqrt; FP32 partial sums over short j-chunks folded
+ *                      into FP64 accumulators.
+ */
+#ifndef G6B200_H
+#define G6B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- GRAPE-6 ABI (include/grape6.h) ---------------------------------- */
+
+/* grape6.h:18-19.  Fixed-point unit exponents of the GRAPE-6 hardware.
+ * Accepted and ignored: this engine chooses its own scaling. */
+void g6_set_tunit_(int *new_tunit);
+void g6_set_xunit_(int *new_xunit);
+
+/* grape6.h:21-22; called at hdyn_grape6.C:164,422,979.  Attach / detach the
+ * engine (device buffers, stream).  Return 0. */
+int g6_open_(int *cluster_id);
+int g6_close_(int *cluster_id);
+
+/* grape6.h:27-28 (sapporo extension; stub in
+ * src/node/dyn/hdyn/stubs/sapporo_stubs.c:17-25 takes a third nmax arg).
+ * Open cluster 0 on device list[0] (a one-GPU engine: entries past the first
+ * are ignored); nmax is a j-capacity hint.  Return 0. */
+int g6_open_special(int ngpu, int *list);
+int g6_open_special2(int ngpu, int *list, int nmax);
+
+/* grape6.h:32-33; hdyn_grape6.C:416-417.  Clear the engine's error state
+ * and drop staged j updates; j-memory is kept (kira reloads it anyway). */
+int g6_reset_(int *cluster_id);
+int g6_reset_fofpga_(int *cluster_id);
+
+/* grape6.h:36; kira_config.C:62,105.  Maximum ni per firsthalf call
+ * (G6B200_NPIPES, default 256).  > 48 tells kira to use the GPU
+ * conventions (self included in neighbour lists, hdyn_grape6.C:2309-2315). */
+int g6_npipes_(void);
+
+/* grape6.h:38; hdyn_grape6.C:516.  Block time the j-particles are
+ * predicted to. */
+void g6_set_ti_(int *cluster_id, double *ti);
+
+/* grape6.h:39-49; hdyn_grape6.C:273-281.  Store j-particle `address`:
+ * time tj, mass, k18 = k/18 (stored, unused by the 3rd-order predictor),
+ * j6 = jerk/6, a2 = acc/2, velocity v and position x.  `index` is the id
+ * compared against firsthalf's index[] to skip self-interaction; kira passes
+ * index == address.  dtj is accepted and ignored.  Return 0, or -1 for a
+ * negative address. */
+int g6_set_j_particle_(int *cluster_id, int *address, int *index,
+                       double *tj, double *dtj, double *mass,
+                       double k18[3], double j6[3], double a2[3],
+                       double v[3], double x[3]);
+
+/* grape6.h:55-66; hdyn_grape6.C:675-677.  Start the force on ni (<= npipes)
+ * i-particles from j-addresses [0, nj).  xi/vi are the i positions and
+ * velocities (already predicted by the caller); aold/j6old/phiold are the
+ * previous acc, full jerk and pot, accepted as scaling hints and unused;
+ * *eps2 is the softening squared; h2[i] > 0 requests i's neighbour list. */
+void g6calc_firsthalf_(int *cluster_id, int *nj, int *ni, int index[],
+                       double xi[][3], double vi[][3], double aold[][3],
+                       double j6old[][3], double phiold[], double *eps2,
+                       double h2[]);
+
+/* grape6.h:68-78.  Wait for the call started by firsthalf; write acc, full
+ * jerk and pot.  Return 0 = OK. */
+int g6calc_lasthalf_(int *cluster_id, int *nj, int *ni, int index[],
+                     double xi[][3], double vi[][3], double *eps2,
+                     double h2[], double acc[][3], double jerk[][3],
+                     double pot[]);
+
+/* grape6.h:80-92; hdyn_grape6.C:687-689.  As lasthalf, plus nnbindex[i],
+ * the address of i's nearest neighbour (0 if it has none). */
+int g6calc_lasthalf2_(int *cluster_id, int *nj, int *ni, int index[],
+                      double xi[][3], double vi[][3], double *eps2,
+                      double h2[], double acc[][3], double jerk[][3],
+                      double pot[], int nnbindex[]);
+
+/* grape6.h:94-95; hdyn_grape6.C:2062-2066.  Make the neighbour lists of the
+ * last call readable.  Return 0 OK, 1 if some list exceeded the engine's
+ * per-pipe capacity (G6B200_NBMAX, default 4096; kira then shrinks h2 and
+ * retries), < 0 on error. */
+int g6_read_neighbour_list_(int *cluster_id);
+int g6_read_neighbour_list_old_(int *cluster_id);
+
+/* grape6.h:97-101; hdyn_grape6.C:2302-2306.  Copy pipe's list (ascending
+ * j-address) into nbl, at most *max_length entries; *nblen = its length.
+ * Return 0, or 1 when the list is longer than *max_length or overflowed the
+ * engine (then *nblen = *max_length, as the GRAPE-6 library does), -1 for a
+ * bad pipe.  With npipes > 48 the list contains i itself. */
+int g6_get_neighbour_list_(int *cluster_id, int *pipe, int *max_length,
+                           int *nblen, int nbl[]);
+
+/* grape6.h:104-105; hdyn_grape6.C:266-271,672-673.  DMA batching of j
+ * writes: staging is always on, so initialize only sizes the staging buffer
+ * and flush pushes staged updates to the device now. */
+int g6_initialize_jp_buffer_(int *clusterid, int *size);
+int g6_flush_jp_buffer_(int *clusterid);
+
+/* Named in the engine's specification but absent from grape6.h (the
+ * reference passes the sphere per i through firsthalf's h2[]).  Sets a
+ * default h2 used for every i when a caller passes h2 == NULL. */
+void g6_set_neighbour_list_sphere_(int *cluster_id, double *h2);
+
+/* ---- Extensions (no counterpart in grape6.h) ------------------------- */
+
+enum { G6B200_FP64 = 0, G6B200_MIXED = 1 };
+
+/* Select the precision mode of an instance (opens it if needed). */
+int g6b200_set_precision(int cluster_id, int mode);
+int g6b200_get_precision(int cluster_id);
+
+/* Maximum ni per firsthalf for this instance (default G6B200_NPIPES or
+ * 256).  g6_npipes_() reports cluster 0's value. */
+int g6b200_set_npipes(int cluster_id, int npipes);
+int g6b200_get_npipes(int cluster_id);
+
+/* Pin the force kernel's launch shape (used by the autotuner and the
+ * benchmarks): il i-lanes per warp (1, 8, 32), r i-particles per thread
+ * (1, or 2 with il = 32), warps per CTA (power of two <= 8), h warps
+ * splitting each CTA's j-tile, nsplit CTAs along j.  il = 0 returns to the
+ * built-in heuristic.  g6b200_get_config reports the shape of the last call
+ * as {il, r, warps, h, nsplit}. */
+int g6b200_set_config(int cluster_id, int il, int r, int warps, int h, int nsplit);
+int g6b200_get_config(int cluster_id, int *out5);
+
+/* Upload n j-particles in one call (SoA-free batched form of
+ * g6_set_j_particle_: arrays of n entries, vectors as [n][3]). */
+int g6b200_set_j_particles(int cluster_id, int n, const int *address,
+                           const int *index, const double *tj,
+                           const double *mass, const double (*k18)[3],
+                           const double (*j6)[3], const double (*a2)[3],
+                           const double (*v)[3], const double (*x)[3]);
+
+/* Counters since open: calls, interactions, j-bytes uploaded, and the
+ * device time of the last call's force kernel in milliseconds. */
+typedef struct {
+    long long calls;
+    long long interactions;
+    long long j_updates;
+    long long h2d_bytes;
+    long long d2h_bytes;
+    double last_force_ms;
+    double last_predict_ms;
+    double last_call_ms;
+} g6b200_stats;
+int g6b200_get_stats(int cluster_id, g6b200_stats *out);
+
+/* Message of the last error on this thread ("" if none). */
+const char *g6b200_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* G6B200_H */

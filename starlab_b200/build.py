@@ -1,0 +1,94 @@
+"""Build the engine library and the oracle's C restatement in-tree.
+
+* ``starlab_b200/lib/libg6b200.so`` -- every ``csrc/*.cu`` compiled by nvcc
+  for sm_100a only (``-gencode arch=compute_100a,code=sm_100a``), linked as
+  one shared library exporting the C ABI of ``include/g6b200.h``.
+* ``oracle/_build/libg6oracle.so`` -- ``oracle/g6_oracle.c`` (test
+  infrastructure) with gcc, FP contraction off.
+
+Usage: ``python -m starlab_b200.build [--verbose] [--ptxas-v]``.
+"""
+import argparse
+import os
+import subprocess
+import sys
+import concurrent.futures as cf
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+REPO = os.path.dirname(PKG)
+CSRC = os.path.join(PKG, "csrc")
+LIBDIR = os.path.join(PKG, "lib")
+OBJDIR = os.path.join(PKG, "_build")
+LIB = os.path.join(LIBDIR, "libg6b200.so")
+ORACLE_SRC = os.path.join(REPO, "oracle", "g6_oracle.c")
+ORACLE_LIB = os.path.join(REPO, "oracle", "_build", "libg6oracle.so")
+
+NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+NVFLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden",
+           "--expt-relaxed-constexpr", "-I" + os.path.join(REPO, "include")]
+
+
+def _newer(out, deps):
+    if not os.path.exists(out):
+        return False
+    t = os.path.getmtime(out)
+    return all(os.path.getmtime(d) <= t for d in deps)
+
+
+def _run(cmd, verbose):
+    if verbose:
+        print(" ".join(cmd))
+    r = subprocess.run(cmd, stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True)
+    if r.returncode != 0:
+        raise RuntimeError("build failed: %s\n%s" % (" ".join(cmd), r.stdout))
+    if verbose and r.stdout.strip():
+        print(r.stdout)
+    return r.stdout
+
+
+def build_engine(verbose=False, ptxas_v=False, force=False):
+    os.makedirs(LIBDIR, exist_ok=True)
+    os.makedirs(OBJDIR, exist_ok=True)
+    srcs = sorted(f for f in os.listdir(CSRC) if f.endswith(".cu"))
+    headers = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".h", ".cuh"))]
+    headers.append(os.path.join(REPO, "include", "g6b200.h"))
+    objs, jobs = [], []
+    for f in srcs:
+        src = os.path.join(CSRC, f)
+        obj = os.path.join(OBJDIR, f[:-3] + ".o")
+        objs.append(obj)
+        if force or not _newer(obj, [src] + headers):
+            cmd = [NVCC] + ARCH + NVFLAGS + (["-Xptxas", "-v"] if ptxas_v else []) + ["-c", src, "-o", obj]
+            jobs.append(cmd)
+    with cf.ThreadPoolExecutor(max(1, min(len(jobs), os.cpu_count() or 4))) as ex:
+        outs = list(ex.map(lambda c: _run(c, verbose), jobs))
+    if ptxas_v:
+        for o in outs:
+            print(o)
+    if force or jobs or not _newer(LIB, objs):
+        _run([NVCC] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcudart"], verbose)
+    return LIB
+
+
+def build_oracle(verbose=False):
+    os.makedirs(os.path.dirname(ORACLE_LIB), exist_ok=True)
+    if not _newer(ORACLE_LIB, [ORACLE_SRC]):
+        _run(["gcc", "-O2", "-fPIC", "-shared", "-ffp-contract=off", "-o", ORACLE_LIB, ORACLE_SRC, "-lm"], verbose)
+    return ORACLE_LIB
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--verbose", action="store_true")
+    ap.add_argument("--ptxas-v", action="store_true")
+    ap.add_argument("--force", action="store_true")
+    a = ap.parse_args(argv)
+    build_engine(a.verbose, a.ptxas_v, a.force)
+    build_oracle(a.verbose)
+    print("built", LIB)
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

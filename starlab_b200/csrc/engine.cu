@@ -1,0 +1,557 @@
+// engine.cu -- host side of one GRAPE-6 engine instance.
+//
+// Call pipeline (one CUDA stream per instance, everything asynchronous
+// until lasthalf):
+//   set_j            host staging, deduplicated per address (last write
+//                    wins), pinned memory
+//   firsthalf        staged j -> device (one copy + scatter kernel);
+//                    predictor, only when the block time, nj, the j-state or
+//                    the fixed-point range changed (kira calls firsthalf once
+//                    per npipes-chunk of a block at the same time);
+//                    i-records -> device; force kernel (+ split reduction);
+//                    neighbour-list compaction when any h2 > 0;
+//                    results -> pinned host memory
+//   lasthalf         wait, check the device status word, copy out.
+// This is the host-side counterpart of the GRAPE-6 library that
+// hdyn_grape6.C drives (send_j_node_to_grape :273, force_by_grape :474-910).
+#include "engine.h"
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+
+namespace g6 {
+
+namespace {
+
+int env_int(const char *name, int dflt) {
+    const char *s = getenv(name);
+    if (!s || !*s) return dflt;
+    return atoi(s);
+}
+
+long long env_ll(const char *name, long long dflt) {
+    const char *s = getenv(name);
+    if (!s || !*s) return dflt;
+    return atoll(s);
+}
+
+int round_up(int x, int m) { return (x + m - 1) / m * m; }
+
+constexpr int kRecMax = 64;  // largest j-record (JRecF64)
+constexpr int kPadTile = 256;
+
+// Output buffer layout for a call with ni i-particles.
+struct OutLayout {
+    size_t status, acc, jerk, pot, nn, total;
+    explicit OutLayout(int ni) {
+        status = 0;
+        acc = 16;
+        jerk = acc + 24 * (size_t)ni;
+        pot = jerk + 24 * (size_t)ni;
+        nn = pot + 8 * (size_t)ni;
+        total = nn + 4 * (size_t)ni;
+    }
+};
+
+}  // namespace
+
+Engine::Engine(int cluster_id) : cluster_id_(cluster_id) {
+    npipes_ = env_int("G6B200_NPIPES", 256);
+    if (npipes_ < 1) npipes_ = 1;
+    nb_cap_ = std::min(std::max(env_int("G6B200_NBMAX", 4096), 16), 8192);
+    const char *pm = getenv("G6B200_PRECISION");
+    if (pm && (!strcmp(pm, "mixed") || !strcmp(pm, "1"))) mode_ = kModeMixed;
+    fault_lasthalf_at_ = env_ll("G6B200_FAULT_LASTHALF", -1);
+    fault_pot_at_ = env_ll("G6B200_FAULT_POT", -1);
+}
+
+Engine::~Engine() { close(); }
+
+int Engine::fail(const char *what, cudaError_t e) {
+    char buf[256];
+    snprintf(buf, sizeof buf, "g6b200[%d]: %s: %s", cluster_id_, what,
+             e == cudaSuccess ? "error" : cudaGetErrorString(e));
+    last_error = buf;
+    return -1;
+}
+
+#define G6_CHECK(call, what)                      \
+    do {                                          \
+        cudaError_t e_ = (call);                  \
+        if (e_ != cudaSuccess) return fail(what, e_); \
+    } while (0)
+
+int Engine::open(int device, int nmax_hint) {
+    if (open_) return 0;
+    device_ = device;
+    G6_CHECK(cudaSetDevice(device_), "cudaSetDevice");
+    G6_CHECK(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "stream");
+    G6_CHECK(cudaDeviceGetAttribute(&num_sms_, cudaDevAttrMultiProcessorCount, device_), "attr");
+    cudaEvent_t *evs[] = {&ev_stage_, &ev_begin_, &ev_pred0_, &ev_pred1_, &ev_force0_, &ev_force1_, &ev_done_};
+    for (cudaEvent_t *e : evs) G6_CHECK(cudaEventCreate(e), "event");
+    stage_cap_ = 16384;
+    G6_CHECK(cudaMallocHost(&h_stage_vals_, sizeof(double) * JF_COUNT * stage_cap_), "pinned stage");
+    G6_CHECK(cudaMallocHost(&h_stage_addr_, sizeof(int) * stage_cap_), "pinned stage");
+    G6_CHECK(cudaMallocHost(&h_stage_index_, sizeof(int) * stage_cap_), "pinned stage");
+    G6_CHECK(cudaMalloc(&d_stage_vals_, sizeof(double) * JF_COUNT * stage_cap_), "stage");
+    G6_CHECK(cudaMalloc(&d_stage_addr_, sizeof(int) * stage_cap_), "stage");
+    G6_CHECK(cudaMalloc(&d_stage_index_, sizeof(int) * stage_cap_), "stage");
+    open_ = true;
+    if (ensure_capacity(std::max(nmax_hint, 1024) - 1)) return -1;
+    return 0;
+}
+
+void Engine::close() {
+    if (!open_) return;
+    cudaSetDevice(device_);
+    cudaStreamSynchronize(stream_);
+    auto dfree = [](void *p) { if (p) cudaFree(p); };
+    auto hfree = [](void *p) { if (p) cudaFreeHost(p); };
+    dfree(d_jraw_); dfree(d_jindex_); dfree(d_jrec_);
+    dfree(d_stage_vals_); dfree(d_stage_addr_); dfree(d_stage_index_);
+    dfree(d_irec_); dfree(d_out_); dfree(d_part_);
+    dfree(d_nb_count_); dfree(d_nb_list_); dfree(d_nb_sorted_); dfree(d_nb_off_);
+    hfree(h_stage_vals_); hfree(h_stage_addr_); hfree(h_stage_index_);
+    hfree(h_irec_); hfree(h_out_); hfree(h_nb_off_); hfree(h_nb_count_);
+    cudaEvent_t evs[] = {ev_stage_, ev_begin_, ev_pred0_, ev_pred1_, ev_force0_, ev_force1_, ev_done_};
+    for (cudaEvent_t e : evs) if (e) cudaEventDestroy(e);
+    cudaStreamDestroy(stream_);
+    d_jraw_ = nullptr; d_jindex_ = nullptr; d_jrec_ = nullptr;
+    d_stage_vals_ = nullptr; d_stage_addr_ = nullptr; d_stage_index_ = nullptr;
+    d_irec_ = nullptr; d_out_ = nullptr; d_part_ = nullptr;
+    d_nb_count_ = nullptr; d_nb_list_ = nullptr; d_nb_sorted_ = nullptr; d_nb_off_ = nullptr;
+    h_stage_vals_ = nullptr; h_stage_addr_ = nullptr; h_stage_index_ = nullptr;
+    h_irec_ = nullptr; h_out_ = nullptr; h_nb_off_ = nullptr; h_nb_count_ = nullptr;
+    ev_stage_ = ev_begin_ = ev_pred0_ = ev_pred1_ = ev_force0_ = ev_force1_ = ev_done_ = nullptr;
+    stream_ = nullptr;
+    cap_ = 0; call_cap_ = 0; part_cap_ = 0; nb_alloc_ = 0;
+    n_staged_ = 0; slot_of_.clear(); nonident_.clear(); n_nonident_ = 0;
+    pred_valid_ = false; pending_ = false; xmax_ = 0; E_ = -1000;
+    open_ = false;
+}
+
+int Engine::reset() {
+    if (!open_) return 0;
+    cudaSetDevice(device_);
+    cudaStreamSynchronize(stream_);
+    cudaGetLastError();  // clear a sticky non-fatal error, if any
+    for (int k = 0; k < n_staged_; ++k) slot_of_[h_stage_addr_[k]] = -1;
+    n_staged_ = 0;
+    pending_ = false;
+    pred_valid_ = false;
+    last_error.clear();
+    return 0;
+}
+
+int Engine::set_npipes(int np) {
+    if (np < 1) return -1;
+    npipes_ = np;
+    return 0;
+}
+
+int Engine::set_mode(int mode) {
+    if (mode != kModeF64 && mode != kModeMixed) return -1;
+    if (mode != mode_) pred_valid_ = false;
+    mode_ = mode;
+    return 0;
+}
+
+int Engine::ensure_capacity(int address) {
+    if (address < cap_) return 0;
+    int ncap = std::max(cap_ * 2, round_up(address + 1, kPadTile));
+    ncap = round_up(ncap, kPadTile);
+    G6_CHECK(cudaSetDevice(device_), "cudaSetDevice");
+    G6_CHECK(cudaStreamSynchronize(stream_), "sync");
+    double *nraw = nullptr;
+    int *nidx = nullptr;
+    void *nrec = nullptr;
+    G6_CHECK(cudaMalloc(&nraw, sizeof(double) * JF_COUNT * (size_t)ncap), "j-memory");
+    G6_CHECK(cudaMalloc(&nidx, sizeof(int) * (size_t)ncap), "j-memory");
+    G6_CHECK(cudaMalloc(&nrec, (size_t)kRecMax * ncap), "j-records");
+    G6_CHECK(cudaMemsetAsync(nraw, 0, sizeof(double) * JF_COUNT * (size_t)ncap, stream_), "memset");
+    G6_CHECK(cudaMemsetAsync(nidx, 0xff, sizeof(int) * (size_t)ncap, stream_), "memset");
+    if (cap_ > 0) {
+        G6_CHECK(cudaMemcpy2DAsync(nraw, sizeof(double) * ncap, d_jraw_, sizeof(double) * cap_,
+                                   sizeof(double) * cap_, JF_COUNT, cudaMemcpyDeviceToDevice, stream_),
+                 "grow copy");
+        G6_CHECK(cudaMemcpyAsync(nidx, d_jindex_, sizeof(int) * cap_, cudaMemcpyDeviceToDevice, stream_),
+                 "grow copy");
+    }
+    G6_CHECK(cudaStreamSynchronize(stream_), "sync");
+    if (d_jraw_) cudaFree(d_jraw_);
+    if (d_jindex_) cudaFree(d_jindex_);
+    if (d_jrec_) cudaFree(d_jrec_);
+    d_jraw_ = nraw;
+    d_jindex_ = nidx;
+    d_jrec_ = nrec;
+    cap_ = ncap;
+    slot_of_.resize(cap_, -1);
+    nonident_.resize(cap_, 0);
+    pred_valid_ = false;
+    return 0;
+}
+
+int Engine::set_j(int address, int index, double tj, double mass, const double *k18,
+                  const double *j6, const double *a2, const double *v, const double *x) {
+    if (address < 0) {
+        last_error = "g6b200: negative j address";
+        return -1;
+    }
+    if (!open_ && open(env_int("G6B200_DEVICE", 0), 0)) return -1;
+    if (ensure_capacity(address)) return -1;
+    if (stage_busy_) {
+        G6_CHECK(cudaEventSynchronize(ev_stage_), "stage wait");
+        stage_busy_ = false;
+    }
+    int slot = slot_of_[address];
+    if (slot < 0) {
+        if (n_staged_ == stage_cap_) {
+            if (flush_j()) return -1;
+            G6_CHECK(cudaEventSynchronize(ev_stage_), "stage wait");
+            stage_busy_ = false;
+        }
+        slot = n_staged_++;
+        slot_of_[address] = slot;
+        h_stage_addr_[slot] = address;
+    }
+    h_stage_index_[slot] = index;
+    double *r = h_stage_vals_ + (size_t)slot * JF_COUNT;
+    r[JF_T] = tj;
+    r[JF_M] = mass;
+    for (int c = 0; c < 3; ++c) {
+        r[JF_X + c] = x[c];
+        r[JF_V + c] = v[c];
+        r[JF_A2 + c] = a2[c];
+        r[JF_J6 + c] = j6[c];
+        r[JF_K18 + c] = k18 ? k18[c] : 0.0;
+        double ax = std::fabs(x[c]);
+        if (ax > xmax_) xmax_ = ax;
+    }
+    bool ni = address != index;
+    if (ni != (bool)nonident_[address]) {
+        nonident_[address] = ni;
+        n_nonident_ += ni ? 1 : -1;
+    }
+    stats_.j_updates++;
+    return 0;
+}
+
+int Engine::flush_j() {
+    if (!open_ || n_staged_ == 0) return 0;
+    G6_CHECK(cudaSetDevice(device_), "cudaSetDevice");
+    const int n = n_staged_;
+    G6_CHECK(cudaMemcpyAsync(d_stage_vals_, h_stage_vals_, sizeof(double) * JF_COUNT * n,
+                             cudaMemcpyHostToDevice, stream_), "stage copy");
+    G6_CHECK(cudaMemcpyAsync(d_stage_addr_, h_stage_addr_, sizeof(int) * n, cudaMemcpyHostToDevice, stream_),
+             "stage copy");
+    G6_CHECK(cudaMemcpyAsync(d_stage_index_, h_stage_index_, sizeof(int) * n, cudaMemcpyHostToDevice, stream_),
+             "stage copy");
+    launch_scatter(stream_, n, d_stage_addr_, d_stage_index_, d_stage_vals_, d_jraw_, d_jindex_, cap_);
+    G6_CHECK(cudaGetLastError(), "scatter launch");
+    G6_CHECK(cudaEventRecord(ev_stage_, stream_), "event");
+    stage_busy_ = true;
+    stats_.h2d_bytes += (long long)n * (JF_COUNT * 8 + 8);
+    for (int k = 0; k < n; ++k) slot_of_[h_stage_addr_[k]] = -1;
+    n_staged_ = 0;
+    pred_valid_ = false;
+    return 0;
+}
+
+int Engine::choose_E(double xmax) const {
+    if (!(xmax > 0) || !std::isfinite(xmax)) return 1;
+    int e = std::ilogb(xmax) + 2;  // xmax < 2^(E-1): a factor-2 margin
+    return std::max(e, -60);
+}
+
+FixedScale Engine::scale() const {
+    FixedScale fs;
+    fs.to_units = std::ldexp(1.0, 23 - E_);
+    fs.hi_unit = std::ldexp(1.0, E_ - 23);
+    fs.lo_unit = std::ldexp(1.0, E_ - 46);
+    return fs;
+}
+
+int Engine::ensure_call_buffers(int ni, bool nb, size_t part_bytes) {
+    if (ni > call_cap_) {
+        int ncap = std::max(ni, npipes_);
+        if (h_irec_) cudaFreeHost(h_irec_);
+        if (d_irec_) cudaFree(d_irec_);
+        if (h_out_) cudaFreeHost(h_out_);
+        if (d_out_) cudaFree(d_out_);
+        h_irec_ = d_irec_ = nullptr;
+        h_out_ = d_out_ = nullptr;
+        OutLayout L(ncap);
+        G6_CHECK(cudaMallocHost(&h_irec_, sizeof(IRec) * ncap), "pinned i");
+        G6_CHECK(cudaMalloc(&d_irec_, sizeof(IRec) * ncap), "i-records");
+        G6_CHECK(cudaMallocHost(&h_out_, L.total), "pinned out");
+        G6_CHECK(cudaMalloc(&d_out_, L.total), "out");
+        call_cap_ = ncap;
+    }
+    if (part_bytes > part_cap_) {
+        if (d_part_) cudaFree(d_part_);
+        d_part_ = nullptr;
+        size_t nb_ = part_bytes + part_bytes / 4;
+        G6_CHECK(cudaMalloc(&d_part_, nb_), "partials");
+        part_cap_ = nb_;
+    }
+    if (nb && nb_alloc_ < call_cap_) {
+        if (d_nb_count_) cudaFree(d_nb_count_);
+        if (d_nb_list_) cudaFree(d_nb_list_);
+        if (d_nb_sorted_) cudaFree(d_nb_sorted_);
+        if (d_nb_off_) cudaFree(d_nb_off_);
+        if (h_nb_off_) cudaFreeHost(h_nb_off_);
+        if (h_nb_count_) cudaFreeHost(h_nb_count_);
+        const int n = call_cap_;
+        G6_CHECK(cudaMalloc(&d_nb_count_, sizeof(int) * n), "nb");
+        G6_CHECK(cudaMalloc(&d_nb_list_, sizeof(int) * (size_t)n * nb_cap_), "nb");
+        G6_CHECK(cudaMalloc(&d_nb_sorted_, sizeof(int) * (size_t)n * nb_cap_), "nb");
+        G6_CHECK(cudaMalloc(&d_nb_off_, sizeof(long long) * (n + 1)), "nb");
+        G6_CHECK(cudaMallocHost(&h_nb_off_, sizeof(long long) * (n + 1)), "nb");
+        G6_CHECK(cudaMallocHost(&h_nb_count_, sizeof(int) * n), "nb");
+        nb_alloc_ = n;
+    }
+    return 0;
+}
+
+int Engine::firsthalf(int nj, int ni, const int *index, const double (*xi)[3], const double (*vi)[3],
+                      double eps2, const double *h2) {
+    call_error_ = false;
+    if (!open_ && open(env_int("G6B200_DEVICE", 0), 0)) {
+        call_error_ = true;
+        return -1;
+    }
+    if (ni < 0 || nj < 0 || ni > npipes_) {
+        char buf[128];
+        snprintf(buf, sizeof buf, "g6b200: bad call sizes ni=%d nj=%d (npipes=%d)", ni, nj, npipes_);
+        last_error = buf;
+        call_error_ = true;
+        return -1;
+    }
+    if (cudaSetDevice(device_) != cudaSuccess) {
+        call_error_ = true;
+        return fail("cudaSetDevice", cudaErrorInvalidDevice);
+    }
+    if (nj > 0 && ensure_capacity(nj - 1)) {
+        call_error_ = true;
+        return -1;
+    }
+    bool nb = false;
+    for (int i = 0; i < ni; ++i) {
+        double hh = h2 ? h2[i] : default_h2_;
+        if (hh > 0) nb = true;
+    }
+    if (ensure_call_buffers(ni, nb, 0)) {
+        call_error_ = true;
+        return -1;
+    }
+    double xm = xmax_;
+    for (int i = 0; i < ni; ++i) {
+        IRec &r = h_irec_[i];
+        for (int c = 0; c < 3; ++c) {
+            r.x[c] = xi[i][c];
+            r.v[c] = vi[i][c];
+            double ax = std::fabs(xi[i][c]);
+            if (ax > xm) xm = ax;
+        }
+        r.h2 = h2 ? h2[i] : default_h2_;
+        r.index = index[i];
+        r.pad = 0;
+    }
+    xmax_ = xm;
+    call_ni_ = ni;
+    call_nj_ = nj;
+    call_eps2_ = eps2;
+    call_nb_ = nb;
+    nb_read_ = false;
+    if (flush_j()) {
+        call_error_ = true;
+        return -1;
+    }
+    int rc = launch_call();
+    if (rc) {
+        call_error_ = true;
+        return rc;
+    }
+    pending_ = true;
+    return 0;
+}
+
+int Engine::launch_call() {
+    const int ni = call_ni_, nj = call_nj_;
+    const int T = tile_size(mode_);
+    const int nj_pad = round_up(nj, T);
+    if (nj_pad > cap_ && ensure_capacity(nj_pad - 1)) return -1;
+    int E = std::max(E_, choose_E(xmax_));
+    if (E != E_) {
+        E_ = E;
+        pred_valid_ = false;
+    }
+    const FixedScale fs = scale();
+    OutLayout L(ni);
+    G6_CHECK(cudaEventRecord(ev_begin_, stream_), "event");
+    G6_CHECK(cudaMemsetAsync(d_out_, 0, 16, stream_), "memset");
+    unsigned *status = reinterpret_cast<unsigned *>(d_out_ + L.status);
+    pred_timed_ = false;
+    if (!pred_valid_ || pred_ti_ != ti_ || pred_nj_ != nj || pred_mode_ != mode_ || pred_E_ != E_) {
+        G6_CHECK(cudaEventRecord(ev_pred0_, stream_), "event");
+        launch_predict(stream_, mode_, d_jraw_, d_jindex_, cap_, nj, nj_pad, ti_, fs, d_jrec_, status);
+        G6_CHECK(cudaGetLastError(), "predict launch");
+        G6_CHECK(cudaEventRecord(ev_pred1_, stream_), "event");
+        pred_timed_ = true;
+        pred_valid_ = true;
+        pred_ti_ = ti_;
+        pred_nj_ = nj;
+        pred_mode_ = mode_;
+        pred_E_ = E_;
+    }
+    if (ni > 0) {
+        G6_CHECK(cudaMemcpyAsync(d_irec_, h_irec_, sizeof(IRec) * ni, cudaMemcpyHostToDevice, stream_),
+                 "i copy");
+        stats_.h2d_bytes += (long long)sizeof(IRec) * ni;
+        ForceConfig cfg = override_.il > 0 ? override_ : choose_config(mode_, ni, nj_pad, num_sms_, call_nb_);
+        if (ensure_call_buffers(ni, call_nb_, partial_bytes(cfg, ni))) return -1;
+        last_cfg_ = cfg;
+        ForceParams p{};
+        p.jrec = d_jrec_;
+        p.nj = nj;
+        p.nj_pad = nj_pad;
+        p.irec = d_irec_;
+        p.ni = ni;
+        p.eps2 = call_eps2_;
+        p.fs = fs;
+        p.part = d_part_;
+        p.out_acc = reinterpret_cast<double *>(d_out_ + L.acc);
+        p.out_jerk = reinterpret_cast<double *>(d_out_ + L.jerk);
+        p.out_pot = reinterpret_cast<double *>(d_out_ + L.pot);
+        p.out_nn = reinterpret_cast<int *>(d_out_ + L.nn);
+        p.nb_count = d_nb_count_;
+        p.nb_list = d_nb_list_;
+        p.nb_cap = nb_cap_;
+        p.include_self = npipes_ > 48;
+        p.status = status;
+        if (call_nb_) G6_CHECK(cudaMemsetAsync(d_nb_count_, 0, sizeof(int) * ni, stream_), "memset");
+        G6_CHECK(cudaEventRecord(ev_force0_, stream_), "event");
+        G6_CHECK(launch_force(stream_, mode_, cfg, p, n_nonident_ == 0, call_nb_), "force launch");
+        G6_CHECK(cudaEventRecord(ev_force1_, stream_), "event");
+        if (call_nb_) {
+            G6_CHECK(launch_nb_compact(stream_, ni, d_nb_count_, d_nb_list_, nb_cap_, d_nb_off_, d_nb_sorted_),
+                     "nb compact");
+            G6_CHECK(cudaMemcpyAsync(h_nb_off_, d_nb_off_, sizeof(long long) * (ni + 1), cudaMemcpyDeviceToHost,
+                                     stream_), "nb copy");
+            G6_CHECK(cudaMemcpyAsync(h_nb_count_, d_nb_count_, sizeof(int) * ni, cudaMemcpyDeviceToHost, stream_),
+                     "nb copy");
+        }
+    } else {
+        G6_CHECK(cudaEventRecord(ev_force0_, stream_), "event");
+        G6_CHECK(cudaEventRecord(ev_force1_, stream_), "event");
+    }
+    G6_CHECK(cudaMemcpyAsync(h_out_, d_out_, L.total, cudaMemcpyDeviceToHost, stream_), "out copy");
+    stats_.d2h_bytes += (long long)L.total;
+    G6_CHECK(cudaEventRecord(ev_done_, stream_), "event");
+    stats_.calls++;
+    stats_.interactions += (long long)ni * nj;
+    return 0;
+}
+
+int Engine::lasthalf(int ni, double (*acc)[3], double (*jerk)[3], double *pot, int *nn) {
+    if (call_error_ || !pending_) {
+        pending_ = false;
+        if (last_error.empty()) last_error = "g6b200: lasthalf without a successful firsthalf";
+        return 1;
+    }
+    pending_ = false;
+    G6_CHECK(cudaSetDevice(device_), "cudaSetDevice");
+    for (int attempt = 0;; ++attempt) {
+        cudaError_t e = cudaEventSynchronize(ev_done_);
+        if (e != cudaSuccess) {
+            fail("device execution", e);
+            return 2;
+        }
+        unsigned status = *reinterpret_cast<unsigned *>(h_out_);
+        if ((status & ST_RANGE) && attempt < 8) {
+            // Fixed-point range exceeded: widen by 4x and recompute.
+            E_ += 2;
+            pred_valid_ = false;
+            if (launch_call()) return 2;
+            continue;
+        }
+        if (status & ST_TMA_TIMEOUT) {
+            last_error = "g6b200: j-tile copy wait timed out on the device";
+            return 3;
+        }
+        if (status & ST_RANGE) {
+            last_error = "g6b200: positions outside the fixed-point range";
+            return 4;
+        }
+        break;
+    }
+    float ms = 0;
+    if (cudaEventElapsedTime(&ms, ev_force0_, ev_force1_) == cudaSuccess) stats_.last_force_ms = ms;
+    if (pred_timed_ && cudaEventElapsedTime(&ms, ev_pred0_, ev_pred1_) == cudaSuccess)
+        stats_.last_predict_ms = ms;
+    else
+        stats_.last_predict_ms = 0;
+    if (cudaEventElapsedTime(&ms, ev_begin_, ev_done_) == cudaSuccess) stats_.last_call_ms = ms;
+    const int n = std::min(ni, call_ni_);
+    OutLayout L(call_ni_);
+    if (acc) memcpy(acc, h_out_ + L.acc, 24 * (size_t)n);
+    if (jerk) memcpy(jerk, h_out_ + L.jerk, 24 * (size_t)n);
+    if (pot) memcpy(pot, h_out_ + L.pot, 8 * (size_t)n);
+    if (nn) memcpy(nn, h_out_ + L.nn, 4 * (size_t)n);
+    ++lasthalf_count_;
+    if (fault_lasthalf_at_ >= 0 && lasthalf_count_ == fault_lasthalf_at_) {
+        last_error = "g6b200: injected lasthalf failure (G6B200_FAULT_LASTHALF)";
+        return 5;
+    }
+    if (fault_pot_at_ >= 0 && lasthalf_count_ == fault_pot_at_ && pot && n > 0) pot[0] = 1.0;
+    return 0;
+}
+
+int Engine::read_neighbours() {
+    if (!open_) return -1;
+    if (!call_nb_) {
+        nb_host_.clear();
+        nb_read_ = true;
+        return 0;
+    }
+    G6_CHECK(cudaSetDevice(device_), "cudaSetDevice");
+    G6_CHECK(cudaEventSynchronize(ev_done_), "wait");
+    const long long total = h_nb_off_[call_ni_];
+    nb_host_.resize((size_t)total);
+    if (total > 0) {
+        G6_CHECK(cudaMemcpy(nb_host_.data(), d_nb_sorted_, sizeof(int) * (size_t)total, cudaMemcpyDeviceToHost),
+                 "nb copy");
+        stats_.d2h_bytes += 4 * total;
+    }
+    nb_read_ = true;
+    for (int i = 0; i < call_ni_; ++i)
+        if (h_nb_count_[i] > nb_cap_) return 1;
+    return 0;
+}
+
+int Engine::get_neighbours(int pipe, int max_length, int *nblen, int *nbl) {
+    if (!nb_read_ || pipe < 0 || pipe >= call_ni_) {
+        if (nblen) *nblen = 0;
+        return -1;
+    }
+    if (!call_nb_) {
+        *nblen = 0;
+        return 0;
+    }
+    const int count = h_nb_count_[pipe];
+    const long long off = h_nb_off_[pipe];
+    const int stored = (int)(h_nb_off_[pipe + 1] - off);
+    if (count > max_length || count > nb_cap_) {
+        const int n = std::min(max_length, stored);
+        if (n > 0) memcpy(nbl, nb_host_.data() + off, sizeof(int) * n);
+        *nblen = max_length;
+        return 1;
+    }
+    if (stored > 0) memcpy(nbl, nb_host_.data() + off, sizeof(int) * stored);
+    *nblen = stored;
+    return 0;
+}
+
+}  // namespace g6

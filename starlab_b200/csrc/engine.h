@@ -1,0 +1,134 @@
+// engine.h -- one GRAPE-6 engine instance (one cluster_id) on one GPU.
+#pragma once
+#include <cuda_runtime.h>
+#include <string>
+#include <vector>
+#include "kernels.h"
+
+namespace g6 {
+
+struct EngineStats {
+    long long calls = 0;
+    long long interactions = 0;
+    long long j_updates = 0;
+    long long h2d_bytes = 0;
+    long long d2h_bytes = 0;
+    double last_force_ms = 0;
+    double last_predict_ms = 0;
+    double last_call_ms = 0;
+};
+
+class Engine {
+  public:
+    explicit Engine(int cluster_id);
+    ~Engine();
+
+    int open(int device, int nmax_hint);  // idempotent
+    void close();
+    int reset();
+    bool is_open() const { return open_; }
+
+    int set_npipes(int np);
+    int npipes() const { return npipes_; }
+    int set_mode(int mode);
+    int mode() const { return mode_; }
+    void set_ti(double ti) { ti_ = ti; }
+    void set_default_h2(double h2) { default_h2_ = h2; }
+    // Force a launch configuration (autotuner / experiments); il=0 clears.
+    void set_config_override(const ForceConfig &c) { override_ = c; }
+
+    int set_j(int address, int index, double tj, double mass, const double *k18,
+              const double *j6, const double *a2, const double *v, const double *x);
+    int flush_j();
+
+    int firsthalf(int nj, int ni, const int *index, const double (*xi)[3],
+                  const double (*vi)[3], double eps2, const double *h2);
+    int lasthalf(int ni, double (*acc)[3], double (*jerk)[3], double *pot, int *nn);
+    int read_neighbours();
+    int get_neighbours(int pipe, int max_length, int *nblen, int *nbl);
+
+    const EngineStats &stats() const { return stats_; }
+    const ForceConfig &last_config() const { return last_cfg_; }
+    std::string last_error;
+
+  private:
+    int ensure_capacity(int address);
+    int ensure_call_buffers(int ni, bool nb, size_t part_bytes);
+    int ensure_nb_buffers();
+    int launch_call();  // predictor (if stale) + force + nb compaction + D2H
+    int fail(const char *what, cudaError_t e);
+    FixedScale scale() const;
+    int choose_E(double xmax) const;
+
+    int cluster_id_;
+    bool open_ = false;
+    int device_ = 0;
+    cudaStream_t stream_ = nullptr;
+    int num_sms_ = 148;
+    int mode_ = kModeF64;
+    int npipes_ = 256;
+    int nb_cap_ = 4096;
+    double ti_ = 0;
+    double default_h2_ = 0;
+    ForceConfig override_{};
+
+    // j-memory
+    int cap_ = 0;
+    double *d_jraw_ = nullptr;
+    int *d_jindex_ = nullptr;
+    void *d_jrec_ = nullptr;
+    int n_nonident_ = 0;
+    std::vector<char> nonident_;
+    double xmax_ = 0;
+    int E_ = -1000;
+
+    // prediction cache
+    bool pred_valid_ = false;
+    double pred_ti_ = 0;
+    int pred_nj_ = -1, pred_mode_ = -1, pred_E_ = 0;
+
+    // j staging (pinned host -> device)
+    int stage_cap_ = 0;
+    int n_staged_ = 0;
+    double *h_stage_vals_ = nullptr;
+    int *h_stage_addr_ = nullptr, *h_stage_index_ = nullptr;
+    double *d_stage_vals_ = nullptr;
+    int *d_stage_addr_ = nullptr, *d_stage_index_ = nullptr;
+    std::vector<int> slot_of_;
+    cudaEvent_t ev_stage_ = nullptr;
+    bool stage_busy_ = false;
+
+    // per-call buffers
+    int call_cap_ = 0;
+    IRec *h_irec_ = nullptr, *d_irec_ = nullptr;
+    unsigned char *h_out_ = nullptr, *d_out_ = nullptr;
+    size_t part_cap_ = 0;
+    Partial *d_part_ = nullptr;
+
+    // neighbour lists
+    int nb_alloc_ = 0;
+    int *d_nb_count_ = nullptr, *d_nb_list_ = nullptr, *d_nb_sorted_ = nullptr;
+    long long *d_nb_off_ = nullptr, *h_nb_off_ = nullptr;
+    int *h_nb_count_ = nullptr;
+    std::vector<int> nb_host_;
+    bool nb_read_ = false;
+
+    // call state
+    bool pending_ = false;
+    int call_ni_ = 0, call_nj_ = 0;
+    double call_eps2_ = 0;
+    bool call_nb_ = false;
+    bool call_error_ = false;
+    ForceConfig last_cfg_{};
+    cudaEvent_t ev_begin_ = nullptr, ev_pred0_ = nullptr, ev_pred1_ = nullptr;
+    cudaEvent_t ev_force0_ = nullptr, ev_force1_ = nullptr, ev_done_ = nullptr;
+    bool pred_timed_ = false;
+
+    // host-side fault injection for the caller's retry paths (tests only)
+    long long fault_lasthalf_at_ = -1, fault_pot_at_ = -1;
+    long long lasthalf_count_ = 0;
+
+    EngineStats stats_;
+};
+
+}  // namespace g6

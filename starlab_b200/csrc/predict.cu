@@ -1,0 +1,113 @@
+// predict.cu -- j-memory scatter and the j-particle predictor.
+//
+// The GRAPE-6 board predicted every j-particle to the block time on board
+// (the CPU equivalent is _dyn_::predict_loworder, include/_dyn_.h:265-299);
+// here one thread per j reads the FP64 SoA j-state (coalesced) and writes
+// one AoS record per j in the precision mode's layout (common.cuh).  The
+// kernel is HBM-bound: 104 B read + 48 B (mixed) or 64 B (FP64) written
+// per j.
+#include "common.cuh"
+#include "kernels.h"
+
+namespace g6 {
+
+// Host staging records -> raw j-state.  One thread per (record, field):
+// reads are contiguous, writes land in 17 SoA rows.
+__global__ void scatter_j_kernel(int n, const int *__restrict__ addr,
+                                 const int *__restrict__ index,
+                                 const double *__restrict__ vals,
+                                 double *__restrict__ jraw, int *__restrict__ jindex,
+                                 int cap) {
+    long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    long long total = (long long)n * JF_COUNT;
+    if (t < total) {
+        int r = (int)(t / JF_COUNT);
+        int f = (int)(t - (long long)r * JF_COUNT);
+        int a = addr[r];
+        jraw[(size_t)f * cap + a] = vals[t];
+        if (f == 0) jindex[a] = index[r];
+    }
+}
+
+__device__ __forceinline__ void predict_one(const double *__restrict__ jraw, int cap, int j,
+                                            double ti, double xp[3], double vp[3], double &m) {
+    double dt = ti - jraw[(size_t)JF_T * cap + j];
+    m = jraw[(size_t)JF_M * cap + j];
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+        double x = jraw[(size_t)(JF_X + c) * cap + j];
+        double v = jraw[(size_t)(JF_V + c) * cap + j];
+        double a2 = jraw[(size_t)(JF_A2 + c) * cap + j];
+        double j6 = jraw[(size_t)(JF_J6 + c) * cap + j];
+        xp[c] = x + dt * (v + dt * (a2 + dt * j6));
+        vp[c] = v + dt * (2.0 * a2 + dt * (3.0 * j6));
+    }
+}
+
+__global__ void predict_mixed_kernel(const double *__restrict__ jraw, const int *__restrict__ jindex,
+                                     int cap, int nj, int nj_pad, double ti, FixedScale fs,
+                                     JRecMixed *__restrict__ out, unsigned *__restrict__ status) {
+    int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= nj_pad) return;
+    JRecMixed r;
+    if (j < nj) {
+        double xp[3], vp[3], m;
+        predict_one(jraw, cap, j, ti, xp, vp, m);
+        float hi[3], lo[3];
+        bool bad = false;
+#pragma unroll
+        for (int c = 0; c < 3; c++) bad |= !to_fixed_split(xp[c], fs, hi[c], lo[c]);
+        if (bad) atomicOr(status, ST_RANGE);
+        r.hi = make_float4(hi[0], hi[1], hi[2], (float)m);
+        r.lo = make_float4(lo[0], lo[1], lo[2], __int_as_float(jindex[j]));
+        r.vel = make_float4((float)vp[0], (float)vp[1], (float)vp[2], 0.f);
+    } else {
+        r.hi = make_float4(kDummyPos, kDummyPos, kDummyPos, 0.f);
+        r.lo = make_float4(0.f, 0.f, 0.f, __int_as_float(-1));
+        r.vel = make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+    out[j] = r;
+}
+
+__global__ void predict_f64_kernel(const double *__restrict__ jraw, const int *__restrict__ jindex,
+                                   int cap, int nj, int nj_pad, double ti,
+                                   JRecF64 *__restrict__ out) {
+    int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= nj_pad) return;
+    JRecF64 r;
+    if (j < nj) {
+        double xp[3], vp[3], m;
+        predict_one(jraw, cap, j, ti, xp, vp, m);
+        r.pos = make_double4(xp[0], xp[1], xp[2], m);
+        r.vel = make_double4(vp[0], vp[1], vp[2], (double)jindex[j]);
+    } else {
+        r.pos = make_double4(kDummyPos, kDummyPos, kDummyPos, 0.0);
+        r.vel = make_double4(0.0, 0.0, 0.0, -1.0);
+    }
+    out[j] = r;
+}
+
+void launch_scatter(cudaStream_t s, int n, const int *addr, const int *index, const double *vals,
+                    double *jraw, int *jindex, int cap) {
+    if (n <= 0) return;
+    long long total = (long long)n * JF_COUNT;
+    int threads = 256;
+    unsigned blocks = (unsigned)((total + threads - 1) / threads);
+    scatter_j_kernel<<<blocks, threads, 0, s>>>(n, addr, index, vals, jraw, jindex, cap);
+}
+
+void launch_predict(cudaStream_t s, int mode, const double *jraw, const int *jindex, int cap,
+                    int nj, int nj_pad, double ti, const FixedScale &fs, void *jrec,
+                    unsigned *status) {
+    if (nj_pad <= 0) return;
+    int threads = 256;
+    int blocks = (nj_pad + threads - 1) / threads;
+    if (mode == kModeMixed)
+        predict_mixed_kernel<<<blocks, threads, 0, s>>>(jraw, jindex, cap, nj, nj_pad, ti, fs,
+                                                         (JRecMixed *)jrec, status);
+    else
+        predict_f64_kernel<<<blocks, threads, 0, s>>>(jraw, jindex, cap, nj, nj_pad, ti,
+                                                       (JRecF64 *)jrec);
+}
+
+}  // namespace g6
