@@ -1,0 +1,388 @@
+#!/usr/bin/env python3
+"""Benchmark of the B200 GRAPE-6 force engine.
+
+Workload (one "step"): a full force sweep of an N = 262144 Plummer sphere
+with a Salpeter mass spectrum (slope -2.35, 0.1-100, total mass 1),
+eps^2 = 1e-8, in the engine's mixed-precision mode: predict all j to the
+step's block time, then acc + jerk + pot + nearest neighbour on every
+particle from every other one, 262144 x 262143 = 6.87e10 pair interactions.
+Inputs are seeded synthetic stand-ins for the reference generators
+(makeplummer | makemass); acc/jerk for the predictor come from one engine
+sweep at t = 0.
+
+Reported (one JSON line on rank 0):
+  value        interactions/s with the j-set resident in HBM, timed on the
+               device with CUDA events on the engine's stream (predictor +
+               i-record build + force + split reduction), L2 flushed (256 MiB
+               write) before every timed step; whole job over all ranks
+  e2e          the same metric through the g6 C ABI with host buffers:
+               every step uploads all j-particles (g6b200_set_j_particles),
+               runs g6calc_firsthalf_/g6calc_lasthalf2_ over all i in npipes
+               chunks from pinned staging, and reads results back
+  roofline     force kernel vs the FP32 pipe: 60 flops per interaction (the
+               acc+jerk convention) / mean force-kernel duration, against
+               SMs x 128 FP32 lanes x 2 x max SM clock
+  cpu_baseline Starlab's own FP64 force loop (oracle/_ref/libref_force.so,
+               hdyn::flat_calculate_acc_and_jerk) on the host cores, on a
+               bounded sample of i
+  latency      p50/p99 of single force calls through the C ABI, ni drawn
+               from a power law (slope -1) on [1, N]
+
+Multi-GPU (torchrun, one rank per GPU): every rank integrates its own
+independent cluster (different seed) -- weak scaling, no collective on the
+data path; timing is the max over ranks.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, REPO)
+
+METRIC = "interactions/s & %FP32 peak (acc+jerk, N=256K); p50/p99 force-call latency"
+FLOPS_PER_INTERACTION = 60
+N_DEFAULT = 262144
+EPS2 = 1e-8
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=N_DEFAULT)
+    ap.add_argument("--e2e-steps", type=int, default=None)
+    ap.add_argument("--latency-calls", type=int, default=200)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------- plumbing
+class Dist:
+    def __init__(self, use_cuda):
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.local = int(os.environ.get("LOCAL_RANK", "0"))
+        self.pg = None
+        self.use_cuda = use_cuda
+        if self.world > 1:
+            import datetime
+            import torch.distributed as dist
+            backend = "nccl" if use_cuda else "gloo"
+            if use_cuda:
+                import torch
+                torch.cuda.set_device(self.local)
+            dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300))
+            self.dist = dist
+
+    def barrier(self):
+        if self.world > 1:
+            self.dist.barrier()
+
+    def max(self, x):
+        if self.world == 1:
+            return float(x)
+        import torch
+        t = torch.tensor([float(x)], dtype=torch.float64, device="cuda" if self.use_cuda else "cpu")
+        self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def close(self):
+        if self.world > 1:
+            self.dist.destroy_process_group()
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during a region."""
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(gpu_index), "--query-gpu=" + self.FIELDS,
+                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                      stdout=self.f, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return None
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=10)
+        except subprocess.TimeoutExpired:
+            self.p.kill()
+        self.f.flush()
+        rows = []
+        for line in open(self.f.name):
+            parts = [s.strip() for s in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                rows.append(dict(sm=float(parts[1]), smax=float(parts[2]), power=float(parts[3]),
+                                 hw=parts[5], hwt=parts[6], swt=parts[7], swp=parts[8]))
+            except ValueError:
+                continue
+        os.unlink(self.f.name)
+        if not rows:
+            return None
+        reasons = set()
+        for r in rows:
+            for key, name in (("hw", "hw_slowdown"), ("hwt", "hw_thermal_slowdown"),
+                              ("swt", "sw_thermal_slowdown"), ("swp", "sw_power_cap")):
+                if r[key].lower().startswith("active"):
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(r["sm"] for r in rows), "sm_max_mhz": max(r["smax"] for r in rows),
+                "power_w_max": max(r["power"] for r in rows), "samples": len(rows), "reasons": sorted(reasons)}
+
+
+def measured_peaks():
+    p = os.path.join(REPO, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        try:
+            return json.load(open(p))
+        except ValueError:
+            return {}
+    return {}
+
+
+def traffic_from_profile():
+    """Per-launch DRAM bytes of the force kernel from the committed ncu
+    summary (profiles/force_mixed_n262144.md: 'traffic_bytes_per_launch')."""
+    p = os.path.join(REPO, "profiles", "force_mixed_n262144.md")
+    if not os.path.exists(p):
+        return None
+    for line in open(p):
+        if line.strip().startswith("traffic_bytes_per_launch:"):
+            try:
+                return float(line.split(":", 1)[1].split()[0])
+            except (ValueError, IndexError):
+                return None
+    return None
+
+
+# ---------------------------------------------------------------- workload
+def make_cluster(n, seed):
+    from starlab_b200 import ics
+    masses = ics.salpeter_masses(n, seed + 1)
+    return ics.plummer(n, seed, masses=masses)
+
+
+def cpu_baseline(n, seed, cores):
+    """Starlab's FP64 force loop on a bounded sample of i (rank 0, N=1)."""
+    m, x, v = make_cluster(n, seed)
+    z = np.zeros((n, 3))
+    try:
+        from oracle.oracle import RefForce
+        ref = RefForce()
+        ni = int(min(n, 640 * cores))
+        ilist = np.linspace(0, n - 1, ni).astype(np.int32)
+        out = ref.force(m, x, v, z, z, 0.0, 0.0, float(np.sqrt(EPS2)), ilist=ilist, nthreads=cores)
+        secs = out["seconds"]
+        return {"value": ni * (n - 1) / secs, "unit": "interactions/s", "cores": cores, "kind": "reference",
+                "sample": "%d i (evenly spaced) x %d j, hdyn::flat_calculate_acc_and_jerk on %d threads; "
+                          "force loop %.2f s" % (ni, n, cores, secs)}
+    except ImportError:
+        from oracle.oracle import G6Oracle
+        o = G6Oracle()
+        ni = 256
+        idx = np.arange(ni, dtype=np.int32)
+        t0 = time.perf_counter()
+        o.force(x, v, m, idx, x[:ni], v[:ni], EPS2)
+        secs = time.perf_counter() - t0
+        return {"value": ni * (n - 1) / secs, "unit": "interactions/s", "cores": 1, "kind": "port",
+                "sample": "%d i x %d j, oracle C restatement, 1 thread" % (ni, n)}
+
+
+def run_reference(args, dist):
+    """--impl reference: the reference's own CPU force path, same metric."""
+    if dist.rank != 0:
+        return
+    cores = os.cpu_count() or 1
+    n = args.n
+    vals = []
+    last = None
+    for k in range(args.warmup + args.steps):
+        r = cpu_baseline(n, 11, cores)
+        if k >= args.warmup:
+            vals.append(r["value"])
+        last = r
+    value = statistics.median(vals)
+    per_step_ms = n * (n - 1) / value * 1e3
+    line = {"metric": METRIC, "impl": "reference", "value": value, "unit": "interactions/s",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": per_step_ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "config": config_of(args, n),
+            "cpu_baseline": {"value": value, "unit": "interactions/s", "cores": last["cores"], "kind": last["kind"],
+                             "sample": last["sample"]},
+            "e2e": {"value": value, "unit": "interactions/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def config_of(args, n):
+    return {"workload": "full force sweep (predict + acc/jerk/pot/nn on all i from all j), "
+                        "N=%d Plummer + Salpeter masses (slope -2.35, 0.1-100), eps2=1e-8, mixed precision" % n,
+            "n": n, "eps2": EPS2, "precision": "mixed (fixed-point positions, FP32 pairs, FP64 sums)",
+            "interactions_per_step": n * (n - 1), "parallelism": "independent cluster per GPU",
+            "l2": "256 MiB buffer written before every timed step (value); e2e re-uploads j and i from host "
+                  "memory every step"}
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        dist = Dist(use_cuda=False)
+        run_reference(args, dist)
+        dist.close()
+        return 0
+    import torch
+    dist = Dist(use_cuda=True)
+    dev = dist.local
+    torch.cuda.set_device(dev)
+    os.environ["G6B200_DEVICE"] = str(dev)
+    from starlab_b200 import G6Engine
+
+    n = args.n
+    seed = 11 + 97 * dist.rank
+    m, x, v = make_cluster(n, seed)
+    z = np.zeros((n, 3))
+    eng = G6Engine(cluster_id=0, precision="mixed", npipes=n)
+    # acc/jerk for the predictor from one sweep at t = 0
+    eng.set_j_particles(0.0, m, z, z, v, x)
+    eng.set_ti(0.0)
+    acc, jerk, pot, nn = eng.sweep(n, eps2=EPS2)
+    eng.set_j_particles(0.0, m, jerk / 6.0, 0.5 * acc, v, x)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    dt = 1.0 / 1024
+
+    def device_step(k):
+        flush.zero_()
+        torch.cuda.synchronize()
+        eng.set_ti(dt * (k + 1))
+        eng.sweep(n, eps2=EPS2, copy_out=False)
+        return eng.stats()
+
+    for k in range(args.warmup):
+        device_step(k)
+    sampler = ClockSampler(dev)
+    dist.barrier()
+    torch.cuda.synchronize()
+    l0 = eng.stats()["launches"]
+    step_ms, force_ms, pred_ms = [], [], []
+    for k in range(args.steps):
+        st = device_step(args.warmup + k)
+        step_ms.append(st["last_call_ms"])
+        force_ms.append(st["last_force_ms"])
+        pred_ms.append(st["last_predict_ms"])
+    torch.cuda.synchronize()
+    dist.barrier()
+    clocks = sampler.stop()
+    launches = eng.stats()["launches"] - l0
+    total_ms = dist.max(sum(step_ms))
+    interactions = n * (n - 1)
+    value = dist.world * interactions * args.steps / (total_ms * 1e-3)
+
+    # ---- e2e through the C ABI with host buffers
+    e2e_steps = args.e2e_steps or max(3, args.steps // 2)
+    npipes = 16384
+    eng2 = G6Engine(cluster_id=1, precision="mixed", npipes=npipes)
+    idx = np.arange(n, dtype=np.int32)
+    a2, j6 = 0.5 * acc, jerk / 6.0
+
+    def e2e_step(k):
+        ti = dt * (k + 1)
+        eng2.set_j_particles(0.0, m, j6, a2, v, x)
+        eng2.set_ti(ti)
+        # host-side i prediction (the caller's job in kira) is outside the
+        # engine; the i arrays are those of the step's block time
+        res = eng2.force(n, idx, xp_h, vp_h, EPS2)
+        return res
+
+    xp_h = x + dt * (v + dt * (a2 + dt * j6))
+    vp_h = v + dt * (2 * a2 + dt * 3 * j6)
+    for k in range(2):
+        e2e_step(k)
+    s0 = eng2.stats()
+    dist.barrier()
+    t0 = time.perf_counter()
+    for k in range(e2e_steps):
+        e2e_step(k)
+    t1 = time.perf_counter()
+    dist.barrier()
+    s1 = eng2.stats()
+    e2e_s = dist.max(t1 - t0)
+    e2e_value = dist.world * interactions * e2e_steps / e2e_s
+    h2d = (s1["h2d_bytes"] - s0["h2d_bytes"]) / e2e_steps
+    d2h = (s1["d2h_bytes"] - s0["d2h_bytes"]) / e2e_steps
+
+    # ---- force-call latency (kira-like i-blocks on the same cluster)
+    rng = np.random.default_rng(5 + dist.rank)
+    lat = []
+    u = rng.uniform(0, 1, args.latency_calls)
+    nis = np.clip(np.exp(u * np.log(n)).astype(int), 1, n)  # p(ni) ~ 1/ni on [1, N]
+    eng3 = G6Engine(cluster_id=2, precision="mixed", npipes=n)
+    eng3.set_j_particles(0.0, m, j6, a2, v, x)
+    eng3.set_ti(dt)
+    for ni in nis[:5]:
+        eng3.force(n, idx[:ni], xp_h[:ni], vp_h[:ni], EPS2)
+    for ni in nis:
+        s = rng.integers(0, n - ni + 1)
+        t0 = time.perf_counter()
+        eng3.calc_firsthalf(n, idx[s:s + ni], xp_h[s:s + ni], vp_h[s:s + ni], EPS2)
+        eng3.calc_lasthalf2()
+        lat.append((time.perf_counter() - t0) * 1e3)
+    lat = np.array(lat)
+
+    if dist.rank == 0:
+        props = torch.cuda.get_device_properties(dev)
+        peaks = measured_peaks()
+        sm_max = float(peaks.get("sm_max_mhz", 1965.0))
+        sms = props.multi_processor_count
+        peak_tflops = sms * 128 * 2 * sm_max * 1e6 / 1e12
+        mean_force = statistics.mean(force_ms)
+        achieved = FLOPS_PER_INTERACTION * interactions / (mean_force * 1e-3) / 1e12
+        traffic = traffic_from_profile()
+        line = {
+            "metric": METRIC, "value": value, "unit": "interactions/s", "n_gpus": dist.world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic", "config": config_of(args, n),
+            "gflops": value * FLOPS_PER_INTERACTION / 1e9,
+            "fp32_peak_frac": achieved / peak_tflops,
+            "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak_tflops, "unit": "TFLOP/s",
+                         "frac": achieved / peak_tflops, "traffic": traffic,
+                         "kernel": "force_kernel (mixed, + split reduction)",
+                         "force_ms_mean": mean_force, "predict_ms_mean": statistics.mean(pred_ms),
+                         "peak_source": "derived: %d SMs x 128 FP32 lanes x 2 flops x %.0f MHz (max SM clock%s)"
+                                        % (sms, sm_max, ", MEASURED_PEAKS.json" if peaks else ", fallback")},
+            "e2e": {"value": e2e_value, "unit": "interactions/s", "h2d_bytes_per_step": int(h2d),
+                    "d2h_bytes_per_step": int(d2h), "steps": e2e_steps, "npipes": npipes,
+                    "ms_per_step": e2e_s / e2e_steps * 1e3},
+            "latency": {"unit": "ms", "calls": int(len(lat)), "p50": float(np.percentile(lat, 50)),
+                        "p99": float(np.percentile(lat, 99)),
+                        "ni_distribution": "power law slope -1 on [1, N]", "path": "g6calc_firsthalf_/lasthalf2_"},
+            "gpu_launches": int(launches),
+            "clocks": clocks,
+        }
+        if dist.world == 1 and not args.no_cpu_baseline:
+            line["cpu_baseline"] = cpu_baseline(n, seed, os.cpu_count() or 1)
+        print(json.dumps(line), flush=True)
+    for e in (eng, eng2, eng3):
+        e.close()
+    dist.close()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -164,8 +164,19 @@ int g6b200_set_j_particles(int cluster_id, int n, const int *address,
                            const double (*j6)[3], const double (*a2)[3],
                            const double (*v)[3], const double (*x)[3]);
 
-/* Counters since open: calls, interactions, j-bytes uploaded, and the
- * device time of the last call's force kernel in milliseconds. */
+/* Self-gravity sweep (blocking): acc, full jerk, pot and nn of the stored
+ * j-particles at addresses [i0, i0+ni) themselves, from all j in [0, nj),
+ * each i predicted to the current ti on the device like the j-side -- the
+ * all-particle pass of an energy evaluation (hdyn_grape6.C:1254-1305) or of
+ * a shared-timestep step, without host i-arrays.  With all four output
+ * pointers NULL the results stay in device memory (timing runs). */
+int g6b200_sweep(int cluster_id, int nj, int i0, int ni, double eps2,
+                 double (*acc)[3], double (*jerk)[3], double *pot, int *nn);
+
+/* Counters since open: calls, interactions, j updates, bytes moved, kernel
+ * launches, and device times (CUDA events on the instance's stream) of the
+ * last call: force kernel (+ split reduction), predictor (0 if the cached
+ * prediction was reused), whole call. */
 typedef struct {
     long long calls;
     long long interactions;
@@ -175,6 +186,7 @@ typedef struct {
     double last_force_ms;
     double last_predict_ms;
     double last_call_ms;
+    long long launches;
 } g6b200_stats;
 int g6b200_get_stats(int cluster_id, g6b200_stats *out);
 

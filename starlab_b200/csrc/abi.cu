@@ -231,6 +231,16 @@ int g6b200_set_j_particles(int cluster_id, int n, const int *address, const int 
     return 0;
 }
 
+int g6b200_sweep(int cluster_id, int nj, int i0, int ni, double eps2, double (*acc)[3], double (*jerk)[3],
+                 double *pot, int *nn) {
+    g6::Engine *e = engine(cluster_id);
+    if (!e) return -1;
+    const bool copy = acc || jerk || pot || nn;
+    int rc = e->sweep(nj, i0, ni, eps2, copy, acc, jerk, pot, nn);
+    if (rc) note(e);
+    return rc;
+}
+
 int g6b200_get_stats(int cluster_id, g6b200_stats *out) {
     const g6::EngineStats &s = engine(cluster_id, false)->stats();
     out->calls = s.calls;
@@ -241,6 +251,7 @@ int g6b200_get_stats(int cluster_id, g6b200_stats *out) {
     out->last_force_ms = s.last_force_ms;
     out->last_predict_ms = s.last_predict_ms;
     out->last_call_ms = s.last_call_ms;
+    out->launches = s.launches;
     return 0;
 }
 

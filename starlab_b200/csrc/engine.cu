@@ -364,6 +364,9 @@ int Engine::firsthalf(int nj, int ni, const int *index, const double (*xi)[3], c
     call_nj_ = nj;
     call_eps2_ = eps2;
     call_nb_ = nb;
+    call_sweep_ = false;
+    call_copy_ = true;
+    call_i0_ = 0;
     nb_read_ = false;
     if (flush_j()) {
         call_error_ = true;
@@ -398,6 +401,7 @@ int Engine::launch_call() {
         G6_CHECK(cudaEventRecord(ev_pred0_, stream_), "event");
         launch_predict(stream_, mode_, d_jraw_, d_jindex_, cap_, nj, nj_pad, ti_, fs, d_jrec_, status);
         G6_CHECK(cudaGetLastError(), "predict launch");
+        stats_.launches++;
         G6_CHECK(cudaEventRecord(ev_pred1_, stream_), "event");
         pred_timed_ = true;
         pred_valid_ = true;
@@ -407,9 +411,15 @@ int Engine::launch_call() {
         pred_E_ = E_;
     }
     if (ni > 0) {
-        G6_CHECK(cudaMemcpyAsync(d_irec_, h_irec_, sizeof(IRec) * ni, cudaMemcpyHostToDevice, stream_),
-                 "i copy");
-        stats_.h2d_bytes += (long long)sizeof(IRec) * ni;
+        if (call_sweep_) {
+            launch_irec_from_j(stream_, d_jraw_, d_jindex_, cap_, call_i0_, ni, ti_, d_irec_);
+            G6_CHECK(cudaGetLastError(), "i-record launch");
+            stats_.launches++;
+        } else {
+            G6_CHECK(cudaMemcpyAsync(d_irec_, h_irec_, sizeof(IRec) * ni, cudaMemcpyHostToDevice, stream_),
+                     "i copy");
+            stats_.h2d_bytes += (long long)sizeof(IRec) * ni;
+        }
         ForceConfig cfg = override_.il > 0 ? override_ : choose_config(mode_, ni, nj_pad, num_sms_, call_nb_);
         if (ensure_call_buffers(ni, call_nb_, partial_bytes(cfg, ni))) return -1;
         last_cfg_ = cfg;
@@ -435,9 +445,11 @@ int Engine::launch_call() {
         G6_CHECK(cudaEventRecord(ev_force0_, stream_), "event");
         G6_CHECK(launch_force(stream_, mode_, cfg, p, n_nonident_ == 0, call_nb_), "force launch");
         G6_CHECK(cudaEventRecord(ev_force1_, stream_), "event");
+        stats_.launches += 1 + (partial_bytes(cfg, ni) > 0 ? 1 : 0);
         if (call_nb_) {
             G6_CHECK(launch_nb_compact(stream_, ni, d_nb_count_, d_nb_list_, nb_cap_, d_nb_off_, d_nb_sorted_),
                      "nb compact");
+            stats_.launches += 2;
             G6_CHECK(cudaMemcpyAsync(h_nb_off_, d_nb_off_, sizeof(long long) * (ni + 1), cudaMemcpyDeviceToHost,
                                      stream_), "nb copy");
             G6_CHECK(cudaMemcpyAsync(h_nb_count_, d_nb_count_, sizeof(int) * ni, cudaMemcpyDeviceToHost, stream_),
@@ -447,8 +459,9 @@ int Engine::launch_call() {
         G6_CHECK(cudaEventRecord(ev_force0_, stream_), "event");
         G6_CHECK(cudaEventRecord(ev_force1_, stream_), "event");
     }
-    G6_CHECK(cudaMemcpyAsync(h_out_, d_out_, L.total, cudaMemcpyDeviceToHost, stream_), "out copy");
-    stats_.d2h_bytes += (long long)L.total;
+    const size_t out_bytes = call_copy_ ? L.total : L.acc;  // status header only when not copying
+    G6_CHECK(cudaMemcpyAsync(h_out_, d_out_, out_bytes, cudaMemcpyDeviceToHost, stream_), "out copy");
+    stats_.d2h_bytes += (long long)out_bytes;
     G6_CHECK(cudaEventRecord(ev_done_, stream_), "event");
     stats_.calls++;
     stats_.interactions += (long long)ni * nj;
@@ -462,6 +475,24 @@ int Engine::lasthalf(int ni, double (*acc)[3], double (*jerk)[3], double *pot, i
         return 1;
     }
     pending_ = false;
+    int rc = wait_call();
+    if (rc) return rc;
+    const int n = std::min(ni, call_ni_);
+    OutLayout L(call_ni_);
+    if (acc) memcpy(acc, h_out_ + L.acc, 24 * (size_t)n);
+    if (jerk) memcpy(jerk, h_out_ + L.jerk, 24 * (size_t)n);
+    if (pot) memcpy(pot, h_out_ + L.pot, 8 * (size_t)n);
+    if (nn) memcpy(nn, h_out_ + L.nn, 4 * (size_t)n);
+    ++lasthalf_count_;
+    if (fault_lasthalf_at_ >= 0 && lasthalf_count_ == fault_lasthalf_at_) {
+        last_error = "g6b200: injected lasthalf failure (G6B200_FAULT_LASTHALF)";
+        return 5;
+    }
+    if (fault_pot_at_ >= 0 && lasthalf_count_ == fault_pot_at_ && pot && n > 0) pot[0] = 1.0;
+    return 0;
+}
+
+int Engine::wait_call() {
     G6_CHECK(cudaSetDevice(device_), "cudaSetDevice");
     for (int attempt = 0;; ++attempt) {
         cudaError_t e = cudaEventSynchronize(ev_done_);
@@ -494,18 +525,42 @@ int Engine::lasthalf(int ni, double (*acc)[3], double (*jerk)[3], double *pot, i
     else
         stats_.last_predict_ms = 0;
     if (cudaEventElapsedTime(&ms, ev_begin_, ev_done_) == cudaSuccess) stats_.last_call_ms = ms;
-    const int n = std::min(ni, call_ni_);
-    OutLayout L(call_ni_);
-    if (acc) memcpy(acc, h_out_ + L.acc, 24 * (size_t)n);
-    if (jerk) memcpy(jerk, h_out_ + L.jerk, 24 * (size_t)n);
-    if (pot) memcpy(pot, h_out_ + L.pot, 8 * (size_t)n);
-    if (nn) memcpy(nn, h_out_ + L.nn, 4 * (size_t)n);
-    ++lasthalf_count_;
-    if (fault_lasthalf_at_ >= 0 && lasthalf_count_ == fault_lasthalf_at_) {
-        last_error = "g6b200: injected lasthalf failure (G6B200_FAULT_LASTHALF)";
-        return 5;
+    return 0;
+}
+
+int Engine::sweep(int nj, int i0, int ni, double eps2, bool copy_out, double (*acc)[3], double (*jerk)[3],
+                  double *pot, int *nn) {
+    if (pending_) {
+        last_error = "g6b200: sweep while a firsthalf call is pending";
+        return -1;
     }
-    if (fault_pot_at_ >= 0 && lasthalf_count_ == fault_pot_at_ && pot && n > 0) pot[0] = 1.0;
+    if (!open_ && open(env_int("G6B200_DEVICE", 0), 0)) return -1;
+    if (ni < 0 || nj < 0 || i0 < 0 || i0 + ni > nj) {
+        last_error = "g6b200: bad sweep range";
+        return -1;
+    }
+    G6_CHECK(cudaSetDevice(device_), "cudaSetDevice");
+    if (nj > 0 && ensure_capacity(nj - 1)) return -1;
+    if (ensure_call_buffers(ni, false, 0)) return -1;
+    call_ni_ = ni;
+    call_nj_ = nj;
+    call_eps2_ = eps2;
+    call_nb_ = false;
+    call_sweep_ = true;
+    call_copy_ = copy_out;
+    call_i0_ = i0;
+    nb_read_ = false;
+    if (flush_j()) return -1;
+    if (launch_call()) return -1;
+    int rc = wait_call();
+    if (rc) return rc;
+    if (copy_out) {
+        OutLayout L(ni);
+        if (acc) memcpy(acc, h_out_ + L.acc, 24 * (size_t)ni);
+        if (jerk) memcpy(jerk, h_out_ + L.jerk, 24 * (size_t)ni);
+        if (pot) memcpy(pot, h_out_ + L.pot, 8 * (size_t)ni);
+        if (nn) memcpy(nn, h_out_ + L.nn, 4 * (size_t)ni);
+    }
     return 0;
 }
 

@@ -16,6 +16,7 @@ struct EngineStats {
     double last_force_ms = 0;
     double last_predict_ms = 0;
     double last_call_ms = 0;
+    long long launches = 0;  // kernels launched by this instance
 };
 
 class Engine {
@@ -44,6 +45,11 @@ class Engine {
     int firsthalf(int nj, int ni, const int *index, const double (*xi)[3],
                   const double (*vi)[3], double eps2, const double *h2);
     int lasthalf(int ni, double (*acc)[3], double (*jerk)[3], double *pot, int *nn);
+    // Self-gravity sweep: forces on the j-addresses [i0, i0+ni) themselves,
+    // predicted on the device (no host i-arrays).  Blocking.  With
+    // copy_out false the results stay in device memory.
+    int sweep(int nj, int i0, int ni, double eps2, bool copy_out, double (*acc)[3], double (*jerk)[3],
+              double *pot, int *nn);
     int read_neighbours();
     int get_neighbours(int pipe, int max_length, int *nblen, int *nbl);
 
@@ -56,6 +62,7 @@ class Engine {
     int ensure_call_buffers(int ni, bool nb, size_t part_bytes);
     int ensure_nb_buffers();
     int launch_call();  // predictor (if stale) + force + nb compaction + D2H
+    int wait_call();    // wait; handle the fixed-point range retry
     int fail(const char *what, cudaError_t e);
     FixedScale scale() const;
     int choose_E(double xmax) const;
@@ -119,6 +126,9 @@ class Engine {
     double call_eps2_ = 0;
     bool call_nb_ = false;
     bool call_error_ = false;
+    bool call_sweep_ = false;
+    bool call_copy_ = true;
+    int call_i0_ = 0;
     ForceConfig last_cfg_{};
     cudaEvent_t ev_begin_ = nullptr, ev_pred0_ = nullptr, ev_pred1_ = nullptr;
     cudaEvent_t ev_force0_ = nullptr, ev_force1_ = nullptr, ev_done_ = nullptr;

@@ -65,6 +65,9 @@ void launch_predict(cudaStream_t s, int mode, const double *jraw, const int *jin
                     int nj, int nj_pad, double ti, const FixedScale &fs, void *jrec,
                     unsigned *status);
 
+void launch_irec_from_j(cudaStream_t s, const double *jraw, const int *jindex, int cap, int i0, int ni,
+                        double ti, IRec *out);
+
 int tile_size(int mode);
 // Choose a launch configuration for ni x nj (heuristic; autotuner overrides).
 ForceConfig choose_config(int mode, int ni, int nj_pad, int num_sms, bool nb);

@@ -87,6 +87,33 @@ __global__ void predict_f64_kernel(const double *__restrict__ jraw, const int *_
     out[j] = r;
 }
 
+// i-records for a self-gravity sweep: the i-particles are j-addresses
+// [i0, i0 + ni), predicted to ti in FP64 exactly as the j-side is.
+__global__ void irec_from_j_kernel(const double *__restrict__ jraw, const int *__restrict__ jindex,
+                                   int cap, int i0, int ni, double ti, IRec *__restrict__ out) {
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= ni) return;
+    int j = i0 + k;
+    double xp[3], vp[3], m;
+    predict_one(jraw, cap, j, ti, xp, vp, m);
+    IRec r;
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+        r.x[c] = xp[c];
+        r.v[c] = vp[c];
+    }
+    r.h2 = 0.0;
+    r.index = jindex[j];
+    r.pad = 0;
+    out[k] = r;
+}
+
+void launch_irec_from_j(cudaStream_t s, const double *jraw, const int *jindex, int cap, int i0, int ni,
+                        double ti, IRec *out) {
+    if (ni <= 0) return;
+    irec_from_j_kernel<<<(ni + 255) / 256, 256, 0, s>>>(jraw, jindex, cap, i0, ni, ti, out);
+}
+
 void launch_scatter(cudaStream_t s, int n, const int *addr, const int *index, const double *vals,
                     double *jraw, int *jindex, int cap) {
     if (n <= 0) return;

@@ -38,7 +38,8 @@ class Stats(ctypes.Structure):
     _fields_ = [("calls", ctypes.c_longlong), ("interactions", ctypes.c_longlong),
                 ("j_updates", ctypes.c_longlong), ("h2d_bytes", ctypes.c_longlong),
                 ("d2h_bytes", ctypes.c_longlong), ("last_force_ms", ctypes.c_double),
-                ("last_predict_ms", ctypes.c_double), ("last_call_ms", ctypes.c_double)]
+                ("last_predict_ms", ctypes.c_double), ("last_call_ms", ctypes.c_double),
+                ("launches", ctypes.c_longlong)]
 
 
 _lib = None
@@ -75,6 +76,7 @@ def load_library(path=None):
         "g6b200_set_config": (I, [I, I, I, I, I, I]), "g6b200_get_config": (I, [I, IP]),
         "g6b200_set_j_particles": (I, [I, I, P, P, P, P, P, P, P, P, P]),
         "g6b200_get_stats": (I, [I, ctypes.POINTER(Stats)]),
+        "g6b200_sweep": (I, [I, I, I, I, D, P, P, P, P]),
         "g6b200_last_error": (ctypes.c_char_p, []),
     }
     for name, (res, args) in sig.items():
@@ -254,6 +256,21 @@ class G6Engine:
             for o, r in zip(outs, res):
                 o[s:e] = r
         return tuple(outs)
+
+    def sweep(self, nj, i0=0, ni=None, eps2=0.0, copy_out=True):
+        """Forces on the stored particles [i0, i0+ni) themselves
+        (g6b200_sweep); returns (acc, jerk, pot, nn) or None when
+        copy_out is False (results left in device memory)."""
+        ni = nj - i0 if ni is None else ni
+        if copy_out:
+            acc, jerk, pot = np.empty((ni, 3)), np.empty((ni, 3)), np.empty(ni)
+            nn = np.empty(ni, dtype=np.int32)
+            rc = self.lib.g6b200_sweep(self.cid, nj, i0, ni, eps2, _ptr(acc), _ptr(jerk), _ptr(pot), _ptr(nn))
+        else:
+            rc = self.lib.g6b200_sweep(self.cid, nj, i0, ni, eps2, None, None, None, None)
+        if rc:
+            self._err("g6b200_sweep", rc)
+        return (acc, jerk, pot, nn) if copy_out else None
 
     # -- neighbour lists -----------------------------------------------
     def read_neighbour_list(self):

@@ -1,0 +1,24 @@
+import os
+import sys
+
+import pytest
+
+REPO = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+if REPO not in sys.path:
+    sys.path.insert(0, REPO)
+
+
+def pytest_configure(config):
+    config.addinivalue_line("markers", "gpu: needs a B200 (runs the CUDA engine)")
+
+
+@pytest.fixture(scope="session")
+def oracle():
+    from oracle.oracle import G6Oracle
+    return G6Oracle()
+
+
+@pytest.fixture(scope="session")
+def ref():
+    from oracle.oracle import RefForce
+    return RefForce()

@@ -1,0 +1,265 @@
+"""Parity of the CUDA engine with the FP64 oracle, through the C ABI.
+
+Single force-call sweep on an N_j = 65536 Plummer snapshot (i-blocks of
+1, 16, 256, 4096 and 65536 particles, neighbour spheres of radius 0.05),
+mixed precision at N = 262144 with a Salpeter mass spectrum, and the edge
+cases of the g6 ABI.  Tolerances (per-particle relative error against the
+FP64 oracle):
+
+    FP64 mode   acc, jerk, pot <= 1e-12;   nn ids identical
+    mixed mode  acc, pot <= 1e-6, jerk <= 1e-5 (max over the sample);
+                nn ids identical except near-ties (second-nearest r^2
+                within 1e-6 relative of the nearest)
+    nb lists    identical in FP64 mode; in mixed mode identical except pairs
+                whose r^2 lies within 1e-6 relative of the sphere radius^2
+"""
+import numpy as np
+import pytest
+
+from helpers import near_tie_mask, rel_err, rel_err_vec, snapshot
+
+pytestmark = pytest.mark.gpu
+
+EPS2 = 1e-3 * 1e-3
+TI = 1.0 / 64
+TOL = {"fp64": dict(acc=1e-12, jerk=1e-12, pot=1e-12),
+       "mixed": dict(acc=1e-6, jerk=1e-5, pot=1e-6)}
+
+_cid = [100]
+
+
+def new_engine(mode, npipes=65536):
+    from starlab_b200 import G6Engine
+    _cid[0] += 1
+    return G6Engine(cluster_id=_cid[0], precision=mode, npipes=npipes)
+
+
+@pytest.fixture(scope="module")
+def c2(oracle):
+    n = 65536
+    m, x, v, a, j = snapshot(n, 7)
+    xp, vp = oracle.predict(TI, 0.0, x, v, 0.5 * a, j / 6.0)
+    return dict(n=n, m=m, x=x, v=v, a=a, j=j, xp=xp, vp=vp)
+
+
+def load(eng, s, tj=0.0):
+    eng.set_j_particles(tj, s["m"], s["j"] / 6.0, 0.5 * s["a"], s["v"], s["x"])
+
+
+def check_forces(mode, got, ref, nn_ok_mask=None):
+    acc, jerk, pot, nn = got
+    ra, rj, rp, rn, _ = ref
+    ea, ej, ep = rel_err_vec(acc, ra), rel_err_vec(jerk, rj), rel_err(pot, rp)
+    tol = TOL[mode]
+    assert ea.max() <= tol["acc"], ("acc", float(np.median(ea)), float(ea.max()))
+    assert ej.max() <= tol["jerk"], ("jerk", float(np.median(ej)), float(ej.max()))
+    assert ep.max() <= tol["pot"], ("pot", float(np.median(ep)), float(ep.max()))
+    bad = nn != rn
+    if nn_ok_mask is not None:
+        bad &= ~nn_ok_mask
+    assert not bad.any(), ("nn mismatch", np.nonzero(bad)[0][:10])
+    return dict(acc_med=float(np.median(ea)), acc_max=float(ea.max()),
+                jerk_med=float(np.median(ej)), jerk_max=float(ej.max()),
+                pot_med=float(np.median(ep)), pot_max=float(ep.max()))
+
+
+@pytest.mark.parametrize("mode", ["fp64", "mixed"])
+def test_single_call_sweep(mode, c2, oracle):
+    eng = new_engine(mode)
+    load(eng, c2)
+    eng.set_ti(TI)
+    n, xp, vp = c2["n"], c2["xp"], c2["vp"]
+    rng = np.random.default_rng(5)
+    for ni in (1, 16, 256, 4096, 65536):
+        idx = np.arange(ni, dtype=np.int32)
+        got = eng.force(n, idx, xp[:ni], vp[:ni], EPS2)
+        samp = idx if ni <= 384 else np.sort(rng.choice(ni, 384, replace=False))
+        ref = oracle.force(xp, vp, c2["m"], samp, xp[samp], vp[samp], EPS2)
+        ties = near_tie_mask(xp, xp[samp], ref[3], index_i=samp) if mode == "mixed" else None
+        check_forces(mode, tuple(g[samp] for g in got), ref, ties)
+    eng.close()
+
+
+@pytest.mark.parametrize("mode", ["fp64", "mixed"])
+def test_neighbour_lists(mode, c2, oracle):
+    eng = new_engine(mode)
+    load(eng, c2)
+    eng.set_ti(TI)
+    n, xp, vp = c2["n"], c2["xp"], c2["vp"]
+    h2 = 0.05 ** 2
+    ni = 256
+    idx = np.arange(1000, 1000 + ni, dtype=np.int32)
+    # half the pipes ask for a list, half do not (h2 = 0)
+    hh = np.where(np.arange(ni) % 2 == 0, h2, 0.0)
+    eng.calc_firsthalf(n, idx, xp[idx], vp[idx], EPS2, hh)
+    eng.calc_lasthalf2()
+    assert eng.read_neighbour_list() == 0
+    lists = oracle.neighbours(xp, idx, xp[idx], hh, include_self=True)
+    total = 0
+    for p in range(ni):
+        rc, nb = eng.get_neighbour_list(p)
+        assert rc == 0
+        want = lists[p]
+        total += len(want)
+        if mode == "fp64":
+            assert np.array_equal(nb, want), p
+        else:
+            diff = np.setxor1d(nb, want)
+            d2 = np.sum((xp[diff] - xp[idx[p]]) ** 2, axis=1)
+            assert np.all(np.abs(d2 - h2) <= 1e-6 * h2), (p, diff)
+            assert np.all(np.diff(nb) > 0)
+        if hh[p] > 0:
+            assert idx[p] in nb  # self is listed when npipes > 48
+    assert total > 500
+    eng.close()
+
+
+def test_neighbour_list_overflow(c2):
+    """A list longer than max_length returns 1 and nblen = max_length."""
+    eng = new_engine("fp64")
+    load(eng, c2)
+    eng.set_ti(TI)
+    n, xp, vp = c2["n"], c2["xp"], c2["vp"]
+    idx = np.arange(4, dtype=np.int32)
+    eng.calc_firsthalf(n, idx, xp[:4], vp[:4], EPS2, np.full(4, 0.3 ** 2))
+    eng.calc_lasthalf2()
+    assert eng.read_neighbour_list() == 0
+    rc, nb = eng.get_neighbour_list(0, max_length=8)
+    assert rc == 1 and len(nb) == 8
+    eng.close()
+
+
+def test_mixed_at_scale_salpeter(oracle):
+    """N = 262144, Salpeter masses, eps2 = 1e-8: sampled parity plus
+    size-independent checks (momentum conservation of the pair sums)."""
+    from starlab_b200 import ics
+    n = 262144
+    masses = ics.salpeter_masses(n, 12)
+    m, x, v, a, j = snapshot(n, 11, masses=masses)
+    eps2 = 1e-8
+    eng = new_engine("mixed", npipes=n)
+    eng.set_j_particles(0.0, m, j / 6.0, 0.5 * a, v, x)
+    eng.set_ti(0.0)
+    idx = np.arange(n, dtype=np.int32)
+    acc, jerk, pot, nn = eng.force(n, idx, x, v, eps2)
+    rng = np.random.default_rng(9)
+    samp = np.sort(rng.choice(n, 256, replace=False))
+    ref = oracle.force(x, v, m, samp, x[samp], v[samp], eps2)
+    ties = near_tie_mask(x, x[samp], ref[3], index_i=samp)
+    check_forces("mixed", (acc[samp], jerk[samp], pot[samp], nn[samp]), ref, ties)
+    # Newton's third law: sum_i m_i a_i = 0 up to pair rounding.
+    mom = np.abs((m[:, None] * acc).sum(0)).max() / (m[:, None] * np.abs(acc)).sum()
+    assert mom < 1e-6, mom
+    eng.close()
+
+
+@pytest.mark.parametrize("mode", ["fp64", "mixed"])
+def test_index_not_address(mode, c2, oracle):
+    """Self-exclusion by index when index != address (general path)."""
+    n = 3000
+    s = {k: (c2[k][:n] if k != "n" else n) for k in ("m", "x", "v", "a", "j", "xp", "vp", "n")}
+    eng = new_engine(mode)
+    ids = (np.arange(n) * 7 + 3).astype(np.int32)
+    eng.set_j_particles(0.0, s["m"], s["j"] / 6.0, 0.5 * s["a"], s["v"], s["x"], index=ids)
+    eng.set_ti(TI)
+    pick = np.array([0, 5, 17, 2999], dtype=np.int32)
+    got = eng.force(n, ids[pick], s["xp"][pick], s["vp"][pick], EPS2)
+    ref = oracle.force(s["xp"], s["vp"], s["m"], ids[pick], s["xp"][pick], s["vp"][pick], EPS2, jindex=ids)
+    check_forces(mode, got, ref)
+    eng.close()
+
+
+@pytest.mark.parametrize("mode", ["fp64", "mixed"])
+def test_ragged_and_tiny(mode, oracle):
+    """nj not a multiple of the tile, ragged ni, nj = 1 and 2, ni = 0."""
+    from starlab_b200 import ics
+    for n, ni in ((1, 1), (2, 2), (3, 3), (257, 257), (1000, 333), (4099, 1025)):
+        m, x, v = ics.plummer(n, 40 + n)
+        eng = new_engine(mode)
+        z = np.zeros((n, 3))
+        eng.set_j_particles(0.0, m, z, z, v, x)
+        eng.set_ti(0.0)
+        idx = np.arange(ni, dtype=np.int32)
+        got = eng.force(n, idx, x[:ni], v[:ni], EPS2)
+        ref = oracle.force(x, v, m, idx, x[:ni], v[:ni], EPS2)
+        if n == 1:
+            assert np.all(got[0] == 0) and np.all(got[2] == 0) and got[3][0] == 0
+        else:
+            check_forces(mode, got, ref)
+        eng.calc_firsthalf(n, idx[:0], x[:0], v[:0], EPS2)
+        assert len(eng.calc_lasthalf2()[0]) == 0
+        eng.close()
+
+
+def test_unsoftened_and_repeated_updates(oracle):
+    """eps2 = 0 with distinct positions; re-setting an address keeps the
+    last write; addresses beyond the initial capacity grow j-memory."""
+    from starlab_b200 import ics
+    n = 5000
+    m, x, v = ics.plummer(n, 77)
+    z = np.zeros((n, 3))
+    eng = new_engine("fp64")
+    eng.set_j_particles(0.0, m, z, z, v + 1.0, x + 1.0)  # stale values first
+    eng.set_j_particles(0.0, m, z, z, v, x)              # then the real ones
+    eng.set_ti(0.0)
+    idx = np.arange(0, n, 97, dtype=np.int32)
+    got = eng.force(n, idx, x[idx], v[idx], 0.0)
+    ref = oracle.force(x, v, m, idx, x[idx], v[idx], 0.0)
+    check_forces("fp64", got, ref)
+    # grow: one particle at address 200000
+    eng.set_j_particle(200000, 0.0, 1e-3, np.zeros(3), np.zeros(3), np.zeros(3), np.zeros(3), np.array([5.0, 0, 0]))
+    eng.close()
+
+
+def test_fixed_point_range_widening(oracle):
+    """A particle far outside the initial range: the engine widens the
+    fixed-point range and recomputes; results stay within tolerance."""
+    from starlab_b200 import ics
+    n = 2048
+    m, x, v = ics.plummer(n, 3)
+    z = np.zeros((n, 3))
+    eng = new_engine("mixed")
+    eng.set_j_particles(0.0, m, z, z, v, x)
+    eng.set_ti(0.0)
+    idx = np.arange(64, dtype=np.int32)
+    eng.force(n, idx, x[idx], v[idx], EPS2)
+    # now move particle 5 far away and give it a large velocity
+    x2 = x.copy()
+    x2[5] = [900.0, -700.0, 1200.0]
+    eng.set_j_particles(0.0, m[5:6], z[:1], z[:1], v[5:6] * 0 + 50.0, x2[5:6], address=[5])
+    v2 = v.copy()
+    v2[5] = 50.0
+    eng.set_ti(0.5)
+    xp, vp = oracle.predict(0.5, 0.0, x2, v2, z, z)
+    got = eng.force(n, idx, xp[idx], vp[idx], EPS2)
+    ref = oracle.force(xp, vp, m, idx, xp[idx], vp[idx], EPS2)
+    check_forces("mixed", got, ref)
+    eng.close()
+
+
+def test_error_conventions(c2):
+    """ni > npipes and lasthalf without firsthalf return nonzero."""
+    from starlab_b200 import G6Error
+    eng = new_engine("fp64", npipes=8)
+    load(eng, c2)
+    eng.set_ti(TI)
+    idx = np.arange(16, dtype=np.int32)
+    eng.calc_firsthalf(c2["n"], idx, c2["xp"][:16], c2["vp"][:16], EPS2)
+    with pytest.raises(G6Error):
+        eng.calc_lasthalf2()
+    with pytest.raises(G6Error):
+        eng.calc_lasthalf2()
+    eng.close()
+
+
+def test_deterministic_repeat(c2):
+    """The same call twice gives bit-identical results."""
+    eng = new_engine("mixed")
+    load(eng, c2)
+    eng.set_ti(TI)
+    idx = np.arange(0, 65536, 3, dtype=np.int32)
+    r1 = eng.force(c2["n"], idx, c2["xp"][idx], c2["vp"][idx], EPS2)
+    r2 = eng.force(c2["n"], idx, c2["xp"][idx], c2["vp"][idx], EPS2)
+    for a, b in zip(r1, r2):
+        assert np.array_equal(a, b)
+    eng.close()
