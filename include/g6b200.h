@@ -190,6 +190,34 @@ typedef struct {
 } g6b200_stats;
 int g6b200_get_stats(int cluster_id, g6b200_stats *out);
 
+/* Allocation-free force evaluation.  No counterpart in the reference: the
+ * GRAPE-6 library owned its board memory, and this entry point exists for
+ * callers of this library that cannot call cudaMalloc -- a host program
+ * whose own allocator or fixed memory budget owns the device, a loop that
+ * must not pay the device-wide synchronisation of cudaMalloc/cudaFree, a
+ * plug-in that is handed only buffers it does not own.  The caller passes
+ * DEVICE pointers for all inputs and outputs: xj, vj [nj][3] and mj [nj]
+ * (positions/velocities already at the block time; no prediction is done),
+ * index_i [ni] (the j-address of each i, skipped in its sum; may be NULL),
+ * xi, vi [ni][3], and outputs acc, jerk [ni][3], pot [ni], nn [ni].  The
+ * sums are FP64 (as G6B200_FP64).  The j-split partial sums use one static
+ * device array of G6B200_NOALLOC_MAX_NI records (80 B each, 2.5 MiB), which
+ * every GPU that loads the library holds until exit; ni beyond
+ * G6B200_NOALLOC_MAX_NI is rejected (returns -1, message in
+ * g6b200_last_error()).  Work is queued on `stream` (a cudaStream_t, NULL =
+ * the legacy default stream) and the call returns without waiting.  The
+ * first call on a device looks up the array's device address there (with
+ * that device current) and should come before any stream capture.  Calls
+ * share the array: two calls whose kernels overlap on the GPU race and give
+ * wrong results; order them on one stream.  Returns 0, -1 (size beyond the
+ * limit), -2 (bad argument), -3 (CUDA error). */
+#define G6B200_NOALLOC_MAX_NI 32768
+int g6b200_force_noalloc(int nj, const double *xj, const double *vj,
+                         const double *mj, int ni, const int *index_i,
+                         const double *xi, const double *vi, double eps2,
+                         double *acc, double *jerk, double *pot, int *nn,
+                         void *stream);
+
 /* Message of the last error on this thread ("" if none). */
 const char *g6b200_last_error(void);
 

@@ -57,6 +57,11 @@ void note(g6::Engine *e) {
 
 }  // namespace
 
+namespace g6 {
+// Lets other translation units of the library set g6b200_last_error().
+void record_error(const std::string &msg) { g_err = msg; }
+}  // namespace g6
+
 extern "C" {
 
 void g6_set_tunit_(int *) {}
