@@ -149,7 +149,7 @@ int g6b200_get_npipes(int cluster_id);
 
 /* Pin the force kernel's launch shape (used by the autotuner and the
  * benchmarks): il i-lanes per warp (1, 8, 32), r i-particles per thread
- * (1, or 2 with il = 32), warps per CTA (power of two <= 8), h warps
+ * (1, or 2 or 4 with il = 32; 4 is mixed mode only), warps per CTA (power of two <= 8), h warps
  * splitting each CTA's j-tile, nsplit CTAs along j.  il = 0 returns to the
  * built-in heuristic.  g6b200_get_config reports the shape of the last call
  * as {il, r, warps, h, nsplit}. */

@@ -199,7 +199,7 @@ int g6b200_set_config(int cluster_id, int il, int r, int warps, int h, int nspli
     c.H = h;
     c.nsplit = nsplit;
     if (il != 0) {
-        bool ok = (il == 1 || il == 8 || il == 32) && (r == 1 || (r == 2 && il == 32)) && warps >= 1 &&
+        bool ok = (il == 1 || il == 8 || il == 32) && (r == 1 || ((r == 2 || r == 4) && il == 32)) && warps >= 1 &&
                   warps <= 8 && (warps & (warps - 1)) == 0 && h >= 1 && warps % h == 0 && nsplit >= 1;
         if (!ok) {
             g_err = "g6b200_set_config: unsupported configuration";

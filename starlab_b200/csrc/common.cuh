@@ -31,6 +31,18 @@ struct __align__(16) JRecMixed {
     float4 vel;   // vx, vy, vz;     w = 0
 };
 
+// Mixed mode, paired layout: 96 B per PAIR of consecutive j (48 B per j),
+// the same fixed-point split as JRecMixed with each component of the two j
+// side by side, so one 8-byte half of a float4 is a ready FP32x2 operand.
+struct __align__(16) JPairMixed {
+    float4 hxy;   // hx0 hx1 hy0 hy1
+    float4 hzm;   // hz0 hz1 m0 m1
+    float4 lxy;   // lx0 lx1 ly0 ly1
+    float4 lzi;   // lz0 lz1 index0 index1 (int bits)
+    float4 vxy;   // vx0 vx1 vy0 vy1
+    float4 vz;    // vz0 vz1 0 0
+};
+
 // FP64 mode: 64 B per j.
 struct __align__(16) JRecF64 {
     double4 pos;  // x, y, z; w = mass

@@ -63,6 +63,8 @@ Engine::Engine(int cluster_id) : cluster_id_(cluster_id) {
     nb_cap_ = std::min(std::max(env_int("G6B200_NBMAX", 4096), 16), 8192);
     const char *pm = getenv("G6B200_PRECISION");
     if (pm && (!strcmp(pm, "mixed") || !strcmp(pm, "1"))) mode_ = kModeMixed;
+    const char *ml = getenv("G6B200_MIXED_LAYOUT");
+    if (ml && !strcmp(ml, "scalar")) mixed_layout_ = kKernMixedDS;
     fault_lasthalf_at_ = env_ll("G6B200_FAULT_LASTHALF", -1);
     fault_pot_at_ = env_ll("G6B200_FAULT_POT", -1);
 }
@@ -383,7 +385,8 @@ int Engine::firsthalf(int nj, int ni, const int *index, const double (*xi)[3], c
 
 int Engine::launch_call() {
     const int ni = call_ni_, nj = call_nj_;
-    const int T = tile_size(mode_);
+    const int km = kmode();
+    const int T = tile_size(km);
     const int nj_pad = round_up(nj, T);
     if (nj_pad > cap_ && ensure_capacity(nj_pad - 1)) return -1;
     int E = std::max(E_, choose_E(xmax_));
@@ -397,9 +400,9 @@ int Engine::launch_call() {
     G6_CHECK(cudaMemsetAsync(d_out_, 0, 16, stream_), "memset");
     unsigned *status = reinterpret_cast<unsigned *>(d_out_ + L.status);
     pred_timed_ = false;
-    if (!pred_valid_ || pred_ti_ != ti_ || pred_nj_ != nj || pred_mode_ != mode_ || pred_E_ != E_) {
+    if (!pred_valid_ || pred_ti_ != ti_ || pred_nj_ != nj || pred_mode_ != km || pred_E_ != E_) {
         G6_CHECK(cudaEventRecord(ev_pred0_, stream_), "event");
-        launch_predict(stream_, mode_, d_jraw_, d_jindex_, cap_, nj, nj_pad, ti_, fs, d_jrec_, status);
+        launch_predict(stream_, km, d_jraw_, d_jindex_, cap_, nj, nj_pad, ti_, fs, d_jrec_, status);
         G6_CHECK(cudaGetLastError(), "predict launch");
         stats_.launches++;
         G6_CHECK(cudaEventRecord(ev_pred1_, stream_), "event");
@@ -407,7 +410,7 @@ int Engine::launch_call() {
         pred_valid_ = true;
         pred_ti_ = ti_;
         pred_nj_ = nj;
-        pred_mode_ = mode_;
+        pred_mode_ = km;
         pred_E_ = E_;
     }
     if (ni > 0) {
@@ -420,7 +423,7 @@ int Engine::launch_call() {
                      "i copy");
             stats_.h2d_bytes += (long long)sizeof(IRec) * ni;
         }
-        ForceConfig cfg = override_.il > 0 ? override_ : choose_config(mode_, ni, nj_pad, num_sms_, call_nb_);
+        ForceConfig cfg = override_.il > 0 ? override_ : choose_config(km, ni, nj_pad, num_sms_, call_nb_);
         if (ensure_call_buffers(ni, call_nb_, partial_bytes(cfg, ni))) return -1;
         last_cfg_ = cfg;
         ForceParams p{};
@@ -443,7 +446,7 @@ int Engine::launch_call() {
         p.status = status;
         if (call_nb_) G6_CHECK(cudaMemsetAsync(d_nb_count_, 0, sizeof(int) * ni, stream_), "memset");
         G6_CHECK(cudaEventRecord(ev_force0_, stream_), "event");
-        G6_CHECK(launch_force(stream_, mode_, cfg, p, n_nonident_ == 0, call_nb_), "force launch");
+        G6_CHECK(launch_force(stream_, km, cfg, p, n_nonident_ == 0, call_nb_), "force launch");
         G6_CHECK(cudaEventRecord(ev_force1_, stream_), "event");
         stats_.launches += 1 + (partial_bytes(cfg, ni) > 0 ? 1 : 0);
         if (call_nb_) {

@@ -73,6 +73,8 @@ class Engine {
     cudaStream_t stream_ = nullptr;
     int num_sms_ = 148;
     int mode_ = kModeF64;
+    int mixed_layout_ = kKernMixedP;  // record layout of the mixed mode
+    int kmode() const { return mode_ == kModeF64 ? kKernF64 : mixed_layout_; }
     int npipes_ = 256;
     int nb_cap_ = 4096;
     double ti_ = 0;

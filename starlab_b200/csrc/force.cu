@@ -22,9 +22,11 @@
 // then over the H warps through shared memory.
 //
 // Mixed mode pair arithmetic is FP32 (exact position differences from the
-// fixed-point split, Newton-refined rsqrt.approx); each thread sums up to
-// kFlush pair terms in FP32 and then folds them into FP64 totals.  FP64 mode
-// does the pair arithmetic and the sums in FP64.
+// fixed-point positions, Newton-refined rsqrt.approx); each thread sums up
+// to kFlush pair terms in FP32 and then folds them into FP64 totals.  The
+// paired layout evaluates two j per FP32x2 instruction (add/mul/fma.f32x2),
+// halving the issue slots per interaction.  FP64 mode does the pair
+// arithmetic and the sums in FP64.
 #include <cfloat>
 #include "common.cuh"
 #include "kernels.h"
@@ -35,27 +37,46 @@ constexpr uint64_t kWaitLimitNs = 1000000000ull;  // 1 s per tile wait
 constexpr int kFlush = 64;                        // FP32 terms per FP64 fold
 constexpr int kMaxWarps = 8;
 
-template <int MODE> struct Traits;
-template <> struct Traits<kModeMixed> {
+// T j per shared-memory tile, held as U records of JPU j each.
+template <int K> struct Traits;
+template <> struct Traits<kKernMixedDS> {
     using JRec = JRecMixed;
-    static constexpr int T = 256;
+    static constexpr int T = 256, JPU = 1, U = T;
 };
-template <> struct Traits<kModeF64> {
+template <> struct Traits<kKernMixedP> {
+    using JRec = JPairMixed;
+    static constexpr int T = 256, JPU = 2, U = T / 2;
+};
+template <> struct Traits<kKernF64> {
     using JRec = JRecF64;
-    static constexpr int T = 128;
+    static constexpr int T = 128, JPU = 1, U = T;
 };
 
-int tile_size(int mode) { return mode == kModeMixed ? Traits<kModeMixed>::T : Traits<kModeF64>::T; }
+int tile_size(int kmode) { return kmode == kKernF64 ? Traits<kKernF64>::T : 256; }
+
+static int units_per_tile(int kmode) { return kmode == kKernMixedP ? Traits<kKernMixedP>::U : tile_size(kmode); }
+
+size_t jrec_bytes(int kmode) {
+    switch (kmode) {
+        case kKernF64: return sizeof(JRecF64);
+        case kKernMixedP: return sizeof(JPairMixed) / 2;
+        default: return sizeof(JRecMixed);
+    }
+}
 
 // ----------------------------------------------------------------------------
 // Per-i register state.
 
-struct StateMixed {
-    float xh, yh, zh, xl, yl, zl, vx, vy, vz, h2;
+struct StateMixedBase {
+    float vx, vy, vz, h2;
     float ax, ay, az, jx, jy, jz, pt;   // FP32 sums since the last fold
     double Ax, Ay, Az, Jx, Jy, Jz, Pt;  // FP64 totals
-    float nr2;
+    float nr2;                          // best r^2 so far
     int nj, idx, i;
+};
+
+struct StateMixed : StateMixedBase {
+    float xh, yh, zh, xl, yl, zl;
 };
 
 struct StateF64 {
@@ -65,19 +86,16 @@ struct StateF64 {
     int nj, idx, i;
 };
 
-template <int MODE> struct StateOf;
-template <> struct StateOf<kModeMixed> { using type = StateMixed; };
-template <> struct StateOf<kModeF64> { using type = StateF64; };
+template <int K> struct StateOf;
+template <> struct StateOf<kKernMixedDS> { using type = StateMixed; };
+template <> struct StateOf<kKernF64> { using type = StateF64; };
 
 __device__ __forceinline__ void nb_push(const ForceParams &p, int i, int j) {
     int k = atomicAdd(&p.nb_count[i], 1);
     if (k < p.nb_cap) p.nb_list[(size_t)i * p.nb_cap + k] = j;
 }
 
-__device__ __forceinline__ void load_i(StateMixed &s, const IRec &q, const ForceParams &p, bool &range_ok) {
-    range_ok &= to_fixed_split(q.x[0], p.fs, s.xh, s.xl);
-    range_ok &= to_fixed_split(q.x[1], p.fs, s.yh, s.yl);
-    range_ok &= to_fixed_split(q.x[2], p.fs, s.zh, s.zl);
+__device__ __forceinline__ void init_mixed(StateMixedBase &s, const IRec &q) {
     s.vx = (float)q.v[0];
     s.vy = (float)q.v[1];
     s.vz = (float)q.v[2];
@@ -87,6 +105,13 @@ __device__ __forceinline__ void load_i(StateMixed &s, const IRec &q, const Force
     s.Ax = s.Ay = s.Az = s.Jx = s.Jy = s.Jz = s.Pt = 0.0;
     s.nr2 = FLT_MAX;
     s.nj = -1;
+}
+
+__device__ __forceinline__ void load_i(StateMixed &s, const IRec &q, const ForceParams &p, bool &range_ok) {
+    range_ok &= to_fixed_split(q.x[0], p.fs, s.xh, s.xl);
+    range_ok &= to_fixed_split(q.x[1], p.fs, s.yh, s.yl);
+    range_ok &= to_fixed_split(q.x[2], p.fs, s.zh, s.zl);
+    init_mixed(s, q);
 }
 
 __device__ __forceinline__ void load_i(StateF64 &s, const IRec &q, const ForceParams &, bool &) {
@@ -103,25 +128,38 @@ __device__ __forceinline__ void load_i(StateF64 &s, const IRec &q, const ForcePa
     s.nj = -1;
 }
 
-// One pair evaluation.  CHK: the tile may hold i itself (compare ids).
-template <bool CHK, bool NB, bool IDENT>
-__device__ __forceinline__ void interact(StateMixed &s, const float4 &hi, const float4 &lo,
-                                         const float4 &ve, int jg, float eps2,
-                                         const ForceParams &p) {
-    const float dx = (hi.x - s.xh) + (lo.x - s.xl);
-    const float dy = (hi.y - s.yh) + (lo.y - s.yl);
-    const float dz = (hi.z - s.zh) + (lo.z - s.zl);
-    const float dvx = ve.x - s.vx;
-    const float dvy = ve.y - s.vy;
-    const float dvz = ve.z - s.vz;
-    const float r2n = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
-    const float rv = fmaf(dz, dvz, fmaf(dy, dvy, dx * dvx));
+// A j-particle as the mixed kernels see it after the shared-memory load.
+struct JMixed {
+    float dx, dy, dz;  // exact position difference rounded to FP32
+    float vx, vy, vz, m;
+    int index;
+};
+
+__device__ __forceinline__ void diff(const StateMixed &s, const JRecMixed &J, JMixed &o) {
+    const float4 hi = J.hi, lo = J.lo, ve = J.vel;
+    o.dx = (hi.x - s.xh) + (lo.x - s.xl);
+    o.dy = (hi.y - s.yh) + (lo.y - s.yl);
+    o.dz = (hi.z - s.zh) + (lo.z - s.zl);
+    o.vx = ve.x;
+    o.vy = ve.y;
+    o.vz = ve.z;
+    o.m = hi.w;
+    o.index = __float_as_int(lo.w);
+}
+
+template <bool CHK, bool NB, bool IDENT, class S>
+__device__ __forceinline__ void interact_mixed(S &s, const JMixed &J, int jg, float eps2, const ForceParams &p) {
+    const float dvx = J.vx - s.vx;
+    const float dvy = J.vy - s.vy;
+    const float dvz = J.vz - s.vz;
+    const float r2n = fmaf(J.dz, J.dz, fmaf(J.dy, J.dy, J.dx * J.dx));
+    const float rv = fmaf(J.dz, dvz, fmaf(J.dy, dvy, J.dx * dvx));
     float r2 = r2n + eps2;
-    float mj = hi.w;
+    float mj = J.m;
     float r2nn = r2n;
     bool self = false;
     if (CHK) {
-        self = IDENT ? (jg == s.idx) : (__float_as_int(lo.w) == s.idx);
+        self = IDENT ? (jg == s.idx) : (J.index == s.idx);
         r2 = self ? 1.f : r2;
         mj = self ? 0.f : mj;
         r2nn = self ? FLT_MAX : r2nn;
@@ -135,12 +173,12 @@ __device__ __forceinline__ void interact(StateMixed &s, const float4 &hi, const 
     const float mr3 = mr * r2inv;
     const float a3 = -3.f * rv * r2inv;
     s.pt -= mr;
-    s.ax = fmaf(mr3, dx, s.ax);
-    s.ay = fmaf(mr3, dy, s.ay);
-    s.az = fmaf(mr3, dz, s.az);
-    s.jx = fmaf(mr3, fmaf(a3, dx, dvx), s.jx);
-    s.jy = fmaf(mr3, fmaf(a3, dy, dvy), s.jy);
-    s.jz = fmaf(mr3, fmaf(a3, dz, dvz), s.jz);
+    s.ax = fmaf(mr3, J.dx, s.ax);
+    s.ay = fmaf(mr3, J.dy, s.ay);
+    s.az = fmaf(mr3, J.dz, s.az);
+    s.jx = fmaf(mr3, fmaf(a3, J.dx, dvx), s.jx);
+    s.jy = fmaf(mr3, fmaf(a3, J.dy, dvy), s.jy);
+    s.jz = fmaf(mr3, fmaf(a3, J.dz, dvz), s.jz);
     if (r2nn < s.nr2) {
         s.nr2 = r2nn;
         s.nj = jg;
@@ -194,7 +232,114 @@ __device__ __forceinline__ void interact(StateF64 &s, const double4 &pos, const 
     }
 }
 
-__device__ __forceinline__ void fold(StateMixed &s) {
+// ---- paired layout: one FP32x2 instruction evaluates i against two j.
+// i-side values are held negated and duplicated in both halves, so every
+// difference is an FP32x2 add of a j-pair and a loop-invariant register pair.
+struct StateMixedP {
+    float2 nxh, nyh, nzh, nxl, nyl, nzl, nvx, nvy, nvz;
+    float h2;
+    float2 ax, ay, az, jx, jy, jz, pm;  // FP32 sums since the last fold; pm = sum m/r
+    double Ax, Ay, Az, Jx, Jy, Jz, Pt;
+    float nr2;
+    int nj, idx, i;
+};
+template <> struct StateOf<kKernMixedP> { using type = StateMixedP; };
+
+__device__ __forceinline__ float2 dup(float v) { return make_float2(v, v); }
+
+__device__ __forceinline__ void load_i(StateMixedP &s, const IRec &q, const ForceParams &p, bool &range_ok) {
+    float h, l;
+    range_ok &= to_fixed_split(q.x[0], p.fs, h, l);
+    s.nxh = dup(-h);
+    s.nxl = dup(-l);
+    range_ok &= to_fixed_split(q.x[1], p.fs, h, l);
+    s.nyh = dup(-h);
+    s.nyl = dup(-l);
+    range_ok &= to_fixed_split(q.x[2], p.fs, h, l);
+    s.nzh = dup(-h);
+    s.nzl = dup(-l);
+    s.nvx = dup(-(float)q.v[0]);
+    s.nvy = dup(-(float)q.v[1]);
+    s.nvz = dup(-(float)q.v[2]);
+    s.h2 = (float)q.h2;
+    s.idx = q.index;
+    s.ax = s.ay = s.az = s.jx = s.jy = s.jz = s.pm = make_float2(0.f, 0.f);
+    s.Ax = s.Ay = s.Az = s.Jx = s.Jy = s.Jz = s.Pt = 0.0;
+    s.nr2 = FLT_MAX;
+    s.nj = -1;
+}
+
+template <bool CHK, bool NB, bool IDENT>
+__device__ __forceinline__ void interact_pair(StateMixedP &s, const JPairMixed &J, int jg0, float2 eps2,
+                                              const ForceParams &p) {
+    const float2 dx = __fadd2_rn(__fadd2_rn(make_float2(J.hxy.x, J.hxy.y), s.nxh),
+                                 __fadd2_rn(make_float2(J.lxy.x, J.lxy.y), s.nxl));
+    const float2 dy = __fadd2_rn(__fadd2_rn(make_float2(J.hxy.z, J.hxy.w), s.nyh),
+                                 __fadd2_rn(make_float2(J.lxy.z, J.lxy.w), s.nyl));
+    const float2 dz = __fadd2_rn(__fadd2_rn(make_float2(J.hzm.x, J.hzm.y), s.nzh),
+                                 __fadd2_rn(make_float2(J.lzi.x, J.lzi.y), s.nzl));
+    const float2 dvx = __fadd2_rn(make_float2(J.vxy.x, J.vxy.y), s.nvx);
+    const float2 dvy = __fadd2_rn(make_float2(J.vxy.z, J.vxy.w), s.nvy);
+    const float2 dvz = __fadd2_rn(make_float2(J.vz.x, J.vz.y), s.nvz);
+    const float2 r2n = __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __fmul2_rn(dx, dx)));
+    const float2 rv = __ffma2_rn(dz, dvz, __ffma2_rn(dy, dvy, __fmul2_rn(dx, dvx)));
+    float2 r2 = __fadd2_rn(r2n, eps2);
+    float2 m = make_float2(J.hzm.z, J.hzm.w);
+    float2 r2nn = r2n;
+    bool self0 = false, self1 = false;
+    if (CHK) {
+        self0 = IDENT ? (jg0 == s.idx) : (__float_as_int(J.lzi.z) == s.idx);
+        self1 = IDENT ? (jg0 + 1 == s.idx) : (__float_as_int(J.lzi.w) == s.idx);
+        r2.x = self0 ? 1.f : r2.x;
+        r2.y = self1 ? 1.f : r2.y;
+        m.x = self0 ? 0.f : m.x;
+        m.y = self1 ? 0.f : m.y;
+        r2nn.x = self0 ? FLT_MAX : r2nn.x;
+        r2nn.y = self1 ? FLT_MAX : r2nn.y;
+    }
+    float2 y = make_float2(rsqrt_approx(r2.x), rsqrt_approx(r2.y));
+    // One Newton-Raphson step: y <- y (1.5 - 0.5 r2 y^2).
+    const float2 nhy = __fmul2_rn(__fmul2_rn(r2, dup(-0.5f)), y);
+    y = __fmul2_rn(y, __ffma2_rn(nhy, y, dup(1.5f)));
+    const float2 r2inv = __fmul2_rn(y, y);
+    const float2 mr = __fmul2_rn(m, y);
+    const float2 mr3 = __fmul2_rn(mr, r2inv);
+    const float2 a3 = __fmul2_rn(__fmul2_rn(rv, dup(-3.f)), r2inv);
+    s.pm = __fadd2_rn(s.pm, mr);
+    s.ax = __ffma2_rn(mr3, dx, s.ax);
+    s.ay = __ffma2_rn(mr3, dy, s.ay);
+    s.az = __ffma2_rn(mr3, dz, s.az);
+    s.jx = __ffma2_rn(mr3, __ffma2_rn(a3, dx, dvx), s.jx);
+    s.jy = __ffma2_rn(mr3, __ffma2_rn(a3, dy, dvy), s.jy);
+    s.jz = __ffma2_rn(mr3, __ffma2_rn(a3, dz, dvz), s.jz);
+    if (r2nn.x < s.nr2) {
+        s.nr2 = r2nn.x;
+        s.nj = jg0;
+    }
+    if (r2nn.y < s.nr2) {
+        s.nr2 = r2nn.y;
+        s.nj = jg0 + 1;
+    }
+    if (NB) {
+        const bool hit0 = CHK && self0 ? (p.include_self && s.h2 > 0.f) : (r2n.x < s.h2);
+        const bool hit1 = CHK && self1 ? (p.include_self && s.h2 > 0.f) : (r2n.y < s.h2);
+        if (hit0) nb_push(p, s.i, jg0);
+        if (hit1) nb_push(p, s.i, jg0 + 1);
+    }
+}
+
+__device__ __forceinline__ void fold(StateMixedP &s) {
+    s.Ax += (double)s.ax.x; s.Ax += (double)s.ax.y;
+    s.Ay += (double)s.ay.x; s.Ay += (double)s.ay.y;
+    s.Az += (double)s.az.x; s.Az += (double)s.az.y;
+    s.Jx += (double)s.jx.x; s.Jx += (double)s.jx.y;
+    s.Jy += (double)s.jy.x; s.Jy += (double)s.jy.y;
+    s.Jz += (double)s.jz.x; s.Jz += (double)s.jz.y;
+    s.Pt -= (double)s.pm.x; s.Pt -= (double)s.pm.y;
+    s.ax = s.ay = s.az = s.jx = s.jy = s.jz = s.pm = make_float2(0.f, 0.f);
+}
+
+__device__ __forceinline__ void fold(StateMixedBase &s) {
     s.Ax += (double)s.ax;
     s.Ay += (double)s.ay;
     s.Az += (double)s.az;
@@ -204,30 +349,43 @@ __device__ __forceinline__ void fold(StateMixed &s) {
     s.Pt += (double)s.pt;
     s.ax = s.ay = s.az = s.jx = s.jy = s.jz = s.pt = 0.f;
 }
-__device__ __forceinline__ void fold(StateF64 &) {}
+
+// Variant bits of the mixed kernels: 2 = inner j-loop unrolled by 4 (else
+// 2).  Unrolling by 4 measured 1.3% faster for the scalar layout and equal
+// for the paired one.
+constexpr int kVarUnroll4 = 2;
 
 // Consume one shared-memory tile: this thread's j are kbase + m*JL.
-template <int MODE, int R, int JL, bool CHK, bool NB, bool IDENT>
-__device__ __forceinline__ void consume_tile(typename StateOf<MODE>::type (&st)[R],
-                                             const typename Traits<MODE>::JRec *S, int kbase,
+template <int K, int R, int JL, bool CHK, bool NB, bool IDENT, int V>
+__device__ __forceinline__ void consume_tile(typename StateOf<K>::type (&st)[R],
+                                             const typename Traits<K>::JRec *S, int kbase,
                                              int per, int tb, const ForceParams &p) {
-    if constexpr (MODE == kModeMixed) {
-        const float eps2 = (float)p.eps2;
-        for (int m0 = 0; m0 < per; m0 += kFlush) {
-            const int m1 = min(m0 + kFlush, per);
-#pragma unroll 2
-            for (int m = m0; m < m1; ++m) {
-                const int k = kbase + m * JL;
-                const float4 hi = S[k].hi;
-                const float4 lo = S[k].lo;
-                const float4 ve = S[k].vel;
+    if constexpr (K == kKernMixedP) {
+        const float2 eps2 = dup((float)p.eps2);
+        constexpr int kFlushPairs = kFlush / 2;
+        for (int m0 = 0; m0 < per; m0 += kFlushPairs) {
+            const int m1 = min(m0 + kFlushPairs, per);
+            if (V & kVarUnroll4) {
+#pragma unroll 4
+                for (int m = m0; m < m1; ++m) {
+                    const int k = kbase + m * JL;
+                    const JPairMixed J = S[k];
 #pragma unroll
-                for (int r = 0; r < R; ++r) interact<CHK, NB, IDENT>(st[r], hi, lo, ve, tb + k, eps2, p);
+                    for (int r = 0; r < R; ++r) interact_pair<CHK, NB, IDENT>(st[r], J, tb + 2 * k, eps2, p);
+                }
+            } else {
+#pragma unroll 2
+                for (int m = m0; m < m1; ++m) {
+                    const int k = kbase + m * JL;
+                    const JPairMixed J = S[k];
+#pragma unroll
+                    for (int r = 0; r < R; ++r) interact_pair<CHK, NB, IDENT>(st[r], J, tb + 2 * k, eps2, p);
+                }
             }
 #pragma unroll
             for (int r = 0; r < R; ++r) fold(st[r]);
         }
-    } else {
+    } else if constexpr (K == kKernF64) {
         const double eps2 = p.eps2;
 #pragma unroll 2
         for (int m = 0; m < per; ++m) {
@@ -236,6 +394,38 @@ __device__ __forceinline__ void consume_tile(typename StateOf<MODE>::type (&st)[
             const double4 vel = S[k].vel;
 #pragma unroll
             for (int r = 0; r < R; ++r) interact<CHK, NB, IDENT>(st[r], pos, vel, tb + k, eps2, p);
+        }
+    } else {
+        const float eps2 = (float)p.eps2;
+        for (int m0 = 0; m0 < per; m0 += kFlush) {
+            const int m1 = min(m0 + kFlush, per);
+            if (V & kVarUnroll4) {
+#pragma unroll 4
+                for (int m = m0; m < m1; ++m) {
+                    const int k = kbase + m * JL;
+                    const auto J = S[k];
+#pragma unroll
+                    for (int r = 0; r < R; ++r) {
+                        JMixed d;
+                        diff(st[r], J, d);
+                        interact_mixed<CHK, NB, IDENT>(st[r], d, tb + k, eps2, p);
+                    }
+                }
+            } else {
+#pragma unroll 2
+                for (int m = m0; m < m1; ++m) {
+                    const int k = kbase + m * JL;
+                    const auto J = S[k];
+#pragma unroll
+                    for (int r = 0; r < R; ++r) {
+                        JMixed d;
+                        diff(st[r], J, d);
+                        interact_mixed<CHK, NB, IDENT>(st[r], d, tb + k, eps2, p);
+                    }
+                }
+            }
+#pragma unroll
+            for (int r = 0; r < R; ++r) fold(st[r]);
         }
     }
 }
@@ -247,7 +437,14 @@ __device__ __forceinline__ void take_min(double &r2, int &j, double o_r2, int o_
     }
 }
 
-__device__ __forceinline__ void to_partial(const StateMixed &s, Partial &q) {
+__device__ __forceinline__ void to_partial(const StateMixedBase &s, Partial &q) {
+    q.acc[0] = s.Ax; q.acc[1] = s.Ay; q.acc[2] = s.Az;
+    q.jerk[0] = s.Jx; q.jerk[1] = s.Jy; q.jerk[2] = s.Jz;
+    q.pot = s.Pt;
+    q.nn_r2 = (double)s.nr2;
+    q.nn_j = s.nj;
+}
+__device__ __forceinline__ void to_partial(const StateMixedP &s, Partial &q) {
     q.acc[0] = s.Ax; q.acc[1] = s.Ay; q.acc[2] = s.Az;
     q.jerk[0] = s.Jx; q.jerk[1] = s.Jy; q.jerk[2] = s.Jz;
     q.pot = s.Pt;
@@ -300,18 +497,24 @@ __device__ __forceinline__ void write_final(const ForceParams &p, int i, const P
     p.out_nn[i] = (q.nn_j < 0 || q.nn_j >= p.nj) ? 0 : q.nn_j;
 }
 
-template <int MODE, int IL, int R, bool NB, bool IDENT>
-__global__ void __launch_bounds__(256, 2) force_kernel(const ForceParams p) {
-    using Tr = Traits<MODE>;
+template <int K, int R> struct MinBlocks {
+    static constexpr int value = R >= 4 ? 1 : 2;
+};
+
+template <int K, int IL, int R, bool NB, bool IDENT, int V>
+__global__ void __launch_bounds__(256, MinBlocks<K, R>::value) force_kernel(const ForceParams p) {
+    using Tr = Traits<K>;
     using JRec = typename Tr::JRec;
-    using State = typename StateOf<MODE>::type;
-    constexpr int T = Tr::T;
+    using State = typename StateOf<K>::type;
+    constexpr int T = Tr::T;     // j per tile
+    constexpr int U = Tr::U;     // records per tile
+    constexpr int JPU = Tr::JPU; // j per record
     constexpr int JL = 32 / IL;
-    constexpr unsigned kTileBytes = T * sizeof(JRec);
+    constexpr unsigned kTileBytes = U * sizeof(JRec);
 
     extern __shared__ __align__(128) unsigned char smem[];
     uint64_t *bars = reinterpret_cast<uint64_t *>(smem);          // [2], never reused
-    JRec *tiles = reinterpret_cast<JRec *>(smem + 128);           // [2][T]
+    JRec *tiles = reinterpret_cast<JRec *>(smem + 128);           // [2][U]
     Partial *red = reinterpret_cast<Partial *>(smem + 128);       // epilogue reuse
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -350,20 +553,20 @@ __global__ void __launch_bounds__(256, 2) force_kernel(const ForceParams p) {
     __syncthreads();
     if (threadIdx.x == 0 && ntiles > 0) {
         mbar_arrive_expect_tx(&bars[0], kTileBytes);
-        bulk_g2s(tiles, jrec + jb, kTileBytes, &bars[0]);
+        bulk_g2s(tiles, jrec + jb / JPU, kTileBytes, &bars[0]);
     }
 
-    const int per = T / (H * JL);
-    const int kbase = h * (T / H) + jl;
+    const int per = U / (H * JL);
+    const int kbase = h * (U / H) + jl;
     bool ok = true;
     for (int t = 0; t < ntiles; ++t) {
         const int b = t & 1;
         if (threadIdx.x == 0 && t + 1 < ntiles) {
             mbar_arrive_expect_tx(&bars[b ^ 1], kTileBytes);
-            bulk_g2s(tiles + (b ^ 1) * T, jrec + jb + (t + 1) * T, kTileBytes, &bars[b ^ 1]);
+            bulk_g2s(tiles + (b ^ 1) * U, jrec + (jb + (t + 1) * T) / JPU, kTileBytes, &bars[b ^ 1]);
         }
         if (ok) ok = mbar_wait_bounded(&bars[b], (t >> 1) & 1, kWaitLimitNs);
-        const JRec *S = tiles + b * T;
+        const JRec *S = tiles + b * U;
         const int tb = jb + t * T;
         bool chk = true;
         if (IDENT) {
@@ -373,9 +576,9 @@ __global__ void __launch_bounds__(256, 2) force_kernel(const ForceParams p) {
             chk = __any_sync(0xffffffffu, mine);
         }
         if (chk)
-            consume_tile<MODE, R, JL, true, NB, IDENT>(st, S, kbase, per, tb, p);
+            consume_tile<K, R, JL, true, NB, IDENT, V>(st, S, kbase, per, tb, p);
         else
-            consume_tile<MODE, R, JL, false, NB, IDENT>(st, S, kbase, per, tb, p);
+            consume_tile<K, R, JL, false, NB, IDENT, V>(st, S, kbase, per, tb, p);
         __syncthreads();
     }
     if (!ok) atomicOr(p.status, ST_TMA_TIMEOUT);
@@ -426,26 +629,32 @@ __global__ void reduce_partials_kernel(const ForceParams p) {
 
 using KernelFn = void (*)(const ForceParams);
 
-template <int MODE, int IL, int R>
+template <int K, int IL, int R>
 static KernelFn pick3(bool nb, bool ident) {
-    if (nb) return ident ? force_kernel<MODE, IL, R, true, true> : force_kernel<MODE, IL, R, true, false>;
-    return ident ? force_kernel<MODE, IL, R, false, true> : force_kernel<MODE, IL, R, false, false>;
+    constexpr int V = kVarUnroll4;
+    if (nb) return ident ? force_kernel<K, IL, R, true, true, V> : force_kernel<K, IL, R, true, false, V>;
+    return ident ? force_kernel<K, IL, R, false, true, V> : force_kernel<K, IL, R, false, false, V>;
 }
 
-template <int MODE>
+template <int K>
 static KernelFn pick2(int il, int r, bool nb, bool ident) {
-    if (il == 32) return r == 2 ? pick3<MODE, 32, 2>(nb, ident) : pick3<MODE, 32, 1>(nb, ident);
-    if (il == 8) return pick3<MODE, 8, 1>(nb, ident);
-    return pick3<MODE, 1, 1>(nb, ident);
+    if (il == 32) {
+        if (K == kKernMixedDS && r == 4) return pick3<K, 32, 4>(nb, ident);
+        if (K != kKernMixedP && r == 2) return pick3<K, 32, 2>(nb, ident);
+        return pick3<K, 32, 1>(nb, ident);
+    }
+    if (il == 8) return pick3<K, 8, 1>(nb, ident);
+    return pick3<K, 1, 1>(nb, ident);
 }
 
-static KernelFn pick(int mode, int il, int r, bool nb, bool ident) {
-    return mode == kModeMixed ? pick2<kModeMixed>(il, r, nb, ident) : pick2<kModeF64>(il, r, nb, ident);
+static KernelFn pick(int kmode, int il, int r, bool nb, bool ident) {
+    if (kmode == kKernMixedP) return pick2<kKernMixedP>(il, r, nb, ident);
+    if (kmode == kKernMixedDS) return pick2<kKernMixedDS>(il, r, nb, ident);
+    return pick2<kKernF64>(il, r, nb, ident);
 }
 
-static size_t smem_bytes(int mode, const ForceConfig &c) {
-    size_t rec = mode == kModeMixed ? sizeof(JRecMixed) : sizeof(JRecF64);
-    size_t tiles = 2 * (size_t)tile_size(mode) * rec;
+static size_t smem_bytes(int kmode, const ForceConfig &c) {
+    size_t tiles = 2 * (size_t)tile_size(kmode) * jrec_bytes(kmode);  // bytes per j x j per tile
     size_t itile = (size_t)(c.warps / c.H) * c.il * c.r;
     size_t red = c.H > 1 ? (size_t)c.H * itile * sizeof(Partial) : 0;
     return 128 + (tiles > red ? tiles : red);
@@ -455,21 +664,25 @@ size_t partial_bytes(const ForceConfig &cfg, int ni) {
     return cfg.nsplit > 1 ? (size_t)cfg.nsplit * ni * sizeof(Partial) : 0;
 }
 
-ForceConfig choose_config(int mode, int ni, int nj_pad, int num_sms, bool nb) {
+ForceConfig choose_config(int kmode, int ni, int nj_pad, int num_sms, bool nb) {
     (void)nb;
     ForceConfig c;
     c.warps = kMaxWarps;
     c.il = ni >= 32 ? 32 : (ni > 1 ? 8 : 1);
     if (c.il == 8 && ni > 8) c.il = 32;
-    c.r = (mode == kModeMixed && c.il == 32 && ni >= 8192) ? 2 : 1;
+    // Register blocking: the scalar mixed layout gains from 2 i per thread;
+    // the paired layout already reuses each loaded j-pair twice and runs out
+    // of registers at 2 (measured: 91 ms vs 95 ms for the N = 262144 sweep).
+    c.r = (kmode == kKernMixedDS && c.il == 32 && ni >= 8192) ? 2 : 1;
     // i-groups per CTA: as many warps on distinct i as there are i's.
     int groups_needed = (ni + c.il * c.r - 1) / (c.il * c.r);
     int G = 1;
     while (G * 2 <= c.warps && G * 2 <= groups_needed) G *= 2;
     c.H = c.warps / G;
-    const int T = tile_size(mode);
+    const int T = tile_size(kmode);
     const int JL = 32 / c.il;
-    while (c.H > 1 && T / (c.H * JL) < 1) c.H /= 2;  // keep >= 1 j per thread per tile
+    const int U = units_per_tile(kmode);
+    while (c.H > 1 && U / (c.H * JL) < 1) c.H /= 2;  // keep >= 1 record per thread per tile
     G = c.warps / c.H;
     const int itile = G * c.il * c.r;
     const int n_itiles = (ni + itile - 1) / itile;
@@ -497,9 +710,9 @@ ForceConfig choose_config(int mode, int ni, int nj_pad, int num_sms, bool nb) {
     return c;
 }
 
-cudaError_t launch_force(cudaStream_t s, int mode, const ForceConfig &cfg, ForceParams p,
+cudaError_t launch_force(cudaStream_t s, int kmode, const ForceConfig &cfg, ForceParams p,
                          bool ident, bool nb) {
-    const int T = tile_size(mode);
+    const int T = tile_size(kmode);
     const int ntiles = p.nj_pad / T;
     if (p.ni <= 0) return cudaSuccess;
     if (ntiles <= 0) {
@@ -515,8 +728,8 @@ cudaError_t launch_force(cudaStream_t s, int mode, const ForceConfig &cfg, Force
     const int itile = G * cfg.il * cfg.r;
     dim3 grid((p.ni + itile - 1) / itile, p.nsplit);
     dim3 block(32 * cfg.warps);
-    KernelFn fn = pick(mode, cfg.il, cfg.r, nb, ident);
-    size_t sm = smem_bytes(mode, cfg);
+    KernelFn fn = pick(kmode, cfg.il, cfg.r, nb, ident);
+    size_t sm = smem_bytes(kmode, cfg);
     fn<<<grid, block, sm, s>>>(p);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;

@@ -5,8 +5,15 @@
 
 namespace g6 {
 
+// Precision modes (public, g6b200_set_precision).
 constexpr int kModeF64 = 0;
 constexpr int kModeMixed = 1;
+// Kernel layouts: the mixed mode has two record layouts with bit-identical
+// pair arithmetic: one j per record (scalar FP32), or pairs of j side by
+// side evaluated with FP32x2 instructions (the default).
+constexpr int kKernF64 = 0;
+constexpr int kKernMixedDS = 1;
+constexpr int kKernMixedP = 3;
 
 // Fixed-point scaling of the mixed mode for position exponent E
 // (all |x| < 2^E): units of the coarse grid and of the fine grid.
@@ -53,7 +60,7 @@ struct ForceParams {
 
 struct ForceConfig {
     int il;       // i-lanes per warp (1, 8, 32)
-    int r;        // i per thread (1, 2)
+    int r;        // i per thread (1, 2, 4; 2 and 4 only with il = 32)
     int warps;    // warps per CTA
     int H;        // j-subranges per CTA
     int nsplit;   // CTAs along j
@@ -61,18 +68,20 @@ struct ForceConfig {
 
 void launch_scatter(cudaStream_t s, int n, const int *addr, const int *index, const double *vals,
                     double *jraw, int *jindex, int cap);
-void launch_predict(cudaStream_t s, int mode, const double *jraw, const int *jindex, int cap,
+void launch_predict(cudaStream_t s, int kmode, const double *jraw, const int *jindex, int cap,
                     int nj, int nj_pad, double ti, const FixedScale &fs, void *jrec,
                     unsigned *status);
 
 void launch_irec_from_j(cudaStream_t s, const double *jraw, const int *jindex, int cap, int i0, int ni,
                         double ti, IRec *out);
 
-int tile_size(int mode);
+// kmode: kKernF64 / kKernMixedDS / kKernMixedP.
+int tile_size(int kmode);
+size_t jrec_bytes(int kmode);
 // Choose a launch configuration for ni x nj (heuristic; autotuner overrides).
-ForceConfig choose_config(int mode, int ni, int nj_pad, int num_sms, bool nb);
+ForceConfig choose_config(int kmode, int ni, int nj_pad, int num_sms, bool nb);
 // Launch force (+ split reduction).  Returns a cudaError_t.
-cudaError_t launch_force(cudaStream_t s, int mode, const ForceConfig &cfg, ForceParams p,
+cudaError_t launch_force(cudaStream_t s, int kmode, const ForceConfig &cfg, ForceParams p,
                          bool ident, bool nb);
 size_t partial_bytes(const ForceConfig &cfg, int ni);
 

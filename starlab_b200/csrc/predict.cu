@@ -69,6 +69,50 @@ __global__ void predict_mixed_kernel(const double *__restrict__ jraw, const int 
     out[j] = r;
 }
 
+// One thread per pair of consecutive j (paired layout, JPairMixed).
+__global__ void predict_pair_kernel(const double *__restrict__ jraw, const int *__restrict__ jindex,
+                                    int cap, int nj, int nj_pad, double ti, FixedScale fs,
+                                    JPairMixed *__restrict__ out, unsigned *__restrict__ status) {
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (2 * q >= nj_pad) return;
+    float hi[2][3], lo[2][3], v[2][3], m[2];
+    int id[2];
+    bool bad = false;
+#pragma unroll
+    for (int u = 0; u < 2; ++u) {
+        const int j = 2 * q + u;
+        if (j < nj) {
+            double xp[3], vp[3], mm;
+            predict_one(jraw, cap, j, ti, xp, vp, mm);
+#pragma unroll
+            for (int c = 0; c < 3; c++) {
+                bad |= !to_fixed_split(xp[c], fs, hi[u][c], lo[u][c]);
+                v[u][c] = (float)vp[c];
+            }
+            m[u] = (float)mm;
+            id[u] = jindex[j];
+        } else {
+#pragma unroll
+            for (int c = 0; c < 3; c++) {
+                hi[u][c] = kDummyPos;
+                lo[u][c] = 0.f;
+                v[u][c] = 0.f;
+            }
+            m[u] = 0.f;
+            id[u] = -1;
+        }
+    }
+    if (bad) atomicOr(status, ST_RANGE);
+    JPairMixed r;
+    r.hxy = make_float4(hi[0][0], hi[1][0], hi[0][1], hi[1][1]);
+    r.hzm = make_float4(hi[0][2], hi[1][2], m[0], m[1]);
+    r.lxy = make_float4(lo[0][0], lo[1][0], lo[0][1], lo[1][1]);
+    r.lzi = make_float4(lo[0][2], lo[1][2], __int_as_float(id[0]), __int_as_float(id[1]));
+    r.vxy = make_float4(v[0][0], v[1][0], v[0][1], v[1][1]);
+    r.vz = make_float4(v[0][2], v[1][2], 0.f, 0.f);
+    out[q] = r;
+}
+
 __global__ void predict_f64_kernel(const double *__restrict__ jraw, const int *__restrict__ jindex,
                                    int cap, int nj, int nj_pad, double ti,
                                    JRecF64 *__restrict__ out) {
@@ -123,15 +167,18 @@ void launch_scatter(cudaStream_t s, int n, const int *addr, const int *index, co
     scatter_j_kernel<<<blocks, threads, 0, s>>>(n, addr, index, vals, jraw, jindex, cap);
 }
 
-void launch_predict(cudaStream_t s, int mode, const double *jraw, const int *jindex, int cap,
+void launch_predict(cudaStream_t s, int kmode, const double *jraw, const int *jindex, int cap,
                     int nj, int nj_pad, double ti, const FixedScale &fs, void *jrec,
                     unsigned *status) {
     if (nj_pad <= 0) return;
     int threads = 256;
     int blocks = (nj_pad + threads - 1) / threads;
-    if (mode == kModeMixed)
+    if (kmode == kKernMixedDS)
         predict_mixed_kernel<<<blocks, threads, 0, s>>>(jraw, jindex, cap, nj, nj_pad, ti, fs,
                                                          (JRecMixed *)jrec, status);
+    else if (kmode == kKernMixedP)
+        predict_pair_kernel<<<(nj_pad / 2 + threads - 1) / threads, threads, 0, s>>>(
+            jraw, jindex, cap, nj, nj_pad, ti, fs, (JPairMixed *)jrec, status);
     else
         predict_f64_kernel<<<blocks, threads, 0, s>>>(jraw, jindex, cap, nj, nj_pad, ti,
                                                        (JRecF64 *)jrec);
