@@ -190,6 +190,48 @@ typedef struct {
 } g6b200_stats;
 int g6b200_get_stats(int cluster_id, g6b200_stats *out);
 
+/* ---- Ensemble of independent clusters (no counterpart in grape6.h) ----
+ *
+ * Many clusters integrated together on one GPU with kira's scheme for its
+ * top-level nodes: 4th-order Hermite predictor/corrector (include/_dyn_.h:
+ * 265-299, hdyn_ev.C:1717-1718), individual power-of-two block steps from an
+ * Aarseth-type criterion with accuracy eta, first steps from 0.01|a|/|j|,
+ * steps capped at 1/16.  State stays on the device; every iteration advances
+ * each unfinished cluster by its own next block, and the force work of all
+ * clusters runs as one persistent launch over a (cluster, i-tile, j-split)
+ * work list (graph-captured).  A cluster's sums depend on that cluster alone,
+ * so its trajectory is bit-identical whether it is integrated alone or with
+ * others (same i-tile shape).  run with per_cluster = 1 instead drives the
+ * same integration through one plain engine call per cluster per block
+ * (host prediction and correction), the baseline the batched path is
+ * measured against. */
+typedef struct g6b200_ensemble g6b200_ensemble;
+typedef struct {
+    double seconds;
+    long long interactions;
+    long long iterations;
+    long long launches;
+    int tuned_h;
+} g6b200_ens_stats;
+g6b200_ensemble *g6b200_ens_create(int nclusters, const int *n, const double *eps2, double eta,
+                                   int precision, int device);
+int g6b200_ens_set_cluster(g6b200_ensemble *h, int c, const double *m, const double (*x)[3],
+                           const double (*v)[3]);
+/* Forces and first steps at t = 0 (after every cluster has been set). */
+int g6b200_ens_start(g6b200_ensemble *h);
+/* Advance every cluster to t_end (a multiple of 1/16, so all particles land
+ * on it exactly).  tune = 1 first times the i-tile shapes on live
+ * iterations and keeps the fastest. */
+int g6b200_ens_run(g6b200_ensemble *h, double t_end, int per_cluster, int tune, g6b200_ens_stats *out);
+/* Kinetic and potential energy of every cluster ([2*nclusters]: ek, ep);
+ * valid when all particles share one time (start, or after a run). */
+int g6b200_ens_energies(g6b200_ensemble *h, double *ek_ep);
+/* State of cluster c (any pointer may be NULL): masses, positions,
+ * velocities, acc, jerk, times and current steps of its particles. */
+int g6b200_ens_get_cluster(g6b200_ensemble *h, int c, double *m, double (*x)[3], double (*v)[3],
+                           double (*acc)[3], double (*jerk)[3], double *t, double *dt);
+void g6b200_ens_destroy(g6b200_ensemble *h);
+
 /* Allocation-free force evaluation.  No counterpart in the reference: the
  * GRAPE-6 library owned its board memory, and this entry point exists for
  * callers of this library that cannot call cudaMalloc -- a host program

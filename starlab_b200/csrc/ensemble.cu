@@ -1,0 +1,927 @@
+// ensemble.cu -- many independent clusters integrated together on one GPU.
+//
+// Each cluster is advanced with the 4th-order Hermite scheme and
+// individual power-of-two block timesteps -- the scheme kira runs for its
+// top-level nodes (kira_int.C:560 integrate_list; predictor
+// include/_dyn_.h:265-299; corrector hdyn_ev.C:1717-1718; Aarseth-type
+// timestep criterion with accuracy parameter eta, hdyn_ev.C:521+).  The
+// j-state of every cluster stays in HBM.  One iteration advances EVERY
+// active cluster by its own next block:
+//
+//   schedule   one CTA per cluster: block time t_b = min(t_i + dt_i), the
+//              ordered list of block members, and the cluster's work item
+//              (a ForceParams: its j-records, i-records, softening,
+//              fixed-point scale, outputs, split plan)
+//   scan       prefix sums of the items' task and i counts
+//   predict    all particles of active clusters to their own t_b (FP64),
+//              j-records in the force kernel's layout, i-records of members
+//   force      ONE persistent launch over the (cluster, i-tile, j-split)
+//              work list of all clusters, then the split reduction
+//   correct    Hermite corrector in FP64 + new timestep, in place
+//
+// The iteration is captured once as a CUDA graph and replayed.  For
+// comparison, run_per_cluster drives the same integration through the plain
+// single-cluster engine (one g6 firsthalf/lasthalf2 call per cluster per
+// block, host-side prediction and correction) -- the way independent kira
+// runs would share the GPU.
+#include <algorithm>
+#include <cfloat>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+#include "common.cuh"
+#include "engine.h"
+#include "kernels.h"
+
+namespace g6 {
+
+struct EnsDev {
+    int nc, ntot;
+    const int *off, *n, *cid;
+    const double *eps2;
+    const FixedScale *fs;
+    const long long *part_off;
+    double *x, *v, *a, *jk, *t, *dt, *m;  // x/v/a/jk: [3][ntot]
+    int *slot;
+    double *tblock;
+    int *count, *ntask;
+    void *jrec;
+    IRec *irec;
+    double *acc1, *jerk1, *pot1;
+    int *nn1;
+    Partial *part;
+    ForceParams *items;
+    int *task0, *ipre, *counter;
+    unsigned *status;
+    int *active;
+    unsigned long long *interactions;
+    double t_end, eta, eta_s, dt_max;
+    int kmode;
+    ForceConfig cfg;
+};
+
+__device__ __forceinline__ void predict_state(const EnsDev &d, int g, double tb, double xp[3], double vp[3]) {
+    const double h = tb - d.t[g];
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+        const double x = d.x[c * d.ntot + g], v = d.v[c * d.ntot + g];
+        const double a2 = 0.5 * d.a[c * d.ntot + g], j6 = d.jk[c * d.ntot + g] * (1.0 / 6.0);
+        xp[c] = x + h * (v + h * (a2 + h * j6));
+        vp[c] = v + h * (2.0 * a2 + h * (3.0 * j6));
+    }
+}
+
+// mode 0: next block; mode 1: every particle at its current time (start of
+// the run, or an energy evaluation when all times are equal).
+__global__ void __launch_bounds__(256) ens_schedule_kernel(EnsDev d, int mode) {
+    __shared__ double s_min[256];
+    __shared__ int s_cnt[256];
+    const int c = blockIdx.x, tid = threadIdx.x;
+    const int n = d.n[c], o = d.off[c], pad_end = d.off[c + 1];
+    double tmin = DBL_MAX;
+    if (mode == 0)
+        for (int i = tid; i < n; i += 256) tmin = fmin(tmin, d.t[o + i] + d.dt[o + i]);
+    s_min[tid] = tmin;
+    __syncthreads();
+    for (int w = 128; w > 0; w >>= 1) {
+        if (tid < w) s_min[tid] = fmin(s_min[tid], s_min[tid + w]);
+        __syncthreads();
+    }
+    const double tb = mode == 0 ? s_min[0] : (n > 0 ? d.t[o] : 0.0);
+    const bool active = n > 0 && (mode != 0 || tb <= d.t_end);
+    const int chunk = (n + 255) / 256;
+    const int b = tid * chunk, e = min(b + chunk, n);
+    int local = 0;
+    for (int i = b; i < e; ++i) local += active && (mode != 0 || d.t[o + i] + d.dt[o + i] == tb);
+    s_cnt[tid] = local;
+    __syncthreads();
+    for (int w = 1; w < 256; w <<= 1) {
+        const int add = tid >= w ? s_cnt[tid - w] : 0;
+        __syncthreads();
+        s_cnt[tid] += add;
+        __syncthreads();
+    }
+    int k = s_cnt[tid] - local;
+    for (int i = b; i < e; ++i) {
+        const bool mem = active && (mode != 0 || d.t[o + i] + d.dt[o + i] == tb);
+        d.slot[o + i] = mem ? k++ : -1;
+    }
+    for (int i = n + tid; i < pad_end - o; i += 256) d.slot[o + i] = -1;
+    if (tid == 0) {
+        const int total = s_cnt[255];
+        d.count[c] = total;
+        d.tblock[c] = tb;
+        ForceParams p{};
+        const size_t jb = d.kmode == kKernF64 ? sizeof(JRecF64) : sizeof(JRecMixed);
+        p.jrec = static_cast<const char *>(d.jrec) + (size_t)o * jb;
+        p.nj = n;
+        p.nj_pad = (n + tile_of(d.kmode) - 1) / tile_of(d.kmode) * tile_of(d.kmode);
+        p.irec = d.irec + o;
+        p.ni = total;
+        p.eps2 = d.eps2[c];
+        p.fs = d.fs[c];
+        p.part = d.part + d.part_off[c];
+        p.out_acc = d.acc1 + 3 * (size_t)o;
+        p.out_jerk = d.jerk1 + 3 * (size_t)o;
+        p.out_pot = d.pot1 + o;
+        p.out_nn = d.nn1 + o;
+        p.status = d.status;
+        int nt = 0;
+        batch_plan(d.kmode, d.cfg, p, nt);
+        d.items[c] = p;
+        d.ntask[c] = nt;
+    }
+}
+
+__global__ void ens_scan_kernel(EnsDev d) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    int t = 0, ii = 0, act = 0;
+    unsigned long long inter = 0;
+    for (int c = 0; c < d.nc; ++c) {
+        d.task0[c] = t;
+        d.ipre[c] = ii;
+        t += d.ntask[c];
+        ii += d.count[c];
+        act += d.count[c] > 0;
+        inter += (unsigned long long)d.count[c] * (unsigned long long)d.n[c];
+    }
+    d.task0[d.nc] = t;
+    d.ipre[d.nc] = ii;
+    *d.active = act;
+    *d.interactions += inter;
+    *d.counter = 0;
+}
+
+// Paired mixed records (one thread per pair) or FP64 records (one thread
+// per particle); i-records for the block members.
+__global__ void ens_predict_kernel(EnsDev d) {
+    const int per = d.kmode == kKernMixedP ? 2 : 1;
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    const int g0 = q * per;
+    if (g0 >= d.ntot) return;
+    const int c = d.cid[g0];
+    if (c < 0 || d.count[c] == 0) return;
+    const int o = d.off[c], n = d.n[c];
+    const double tb = d.tblock[c];
+    float hi[2][3], lo[2][3], vv[2][3], mm[2];
+    int id[2];
+    bool bad = false;
+    for (int u = 0; u < per; ++u) {
+        const int g = g0 + u, i = g - o;
+        if (i < n) {
+            double xp[3], vp[3];
+            predict_state(d, g, tb, xp, vp);
+            const int s = d.slot[g];
+            if (s >= 0) {
+                IRec r;
+                for (int k = 0; k < 3; ++k) {
+                    r.x[k] = xp[k];
+                    r.v[k] = vp[k];
+                }
+                r.h2 = 0.0;
+                r.index = i;
+                r.pad = 0;
+                d.irec[o + s] = r;
+            }
+            if (d.kmode == kKernF64) {
+                JRecF64 rec;
+                rec.pos = make_double4(xp[0], xp[1], xp[2], d.m[g]);
+                rec.vel = make_double4(vp[0], vp[1], vp[2], (double)i);
+                reinterpret_cast<JRecF64 *>(d.jrec)[g] = rec;
+            } else {
+                for (int k = 0; k < 3; ++k) {
+                    bad |= !to_fixed_split(xp[k], d.fs[c], hi[u][k], lo[u][k]);
+                    vv[u][k] = (float)vp[k];
+                }
+                mm[u] = (float)d.m[g];
+                id[u] = i;
+            }
+        } else if (d.kmode == kKernF64) {
+            JRecF64 rec;
+            rec.pos = make_double4(kDummyPos, kDummyPos, kDummyPos, 0.0);
+            rec.vel = make_double4(0.0, 0.0, 0.0, -1.0);
+            reinterpret_cast<JRecF64 *>(d.jrec)[g] = rec;
+        } else {
+            for (int k = 0; k < 3; ++k) {
+                hi[u][k] = kDummyPos;
+                lo[u][k] = 0.f;
+                vv[u][k] = 0.f;
+            }
+            mm[u] = 0.f;
+            id[u] = -1;
+        }
+    }
+    if (bad) atomicOr(d.status, ST_RANGE);
+    if (d.kmode == kKernMixedP) {
+        JPairMixed r;
+        r.hxy = make_float4(hi[0][0], hi[1][0], hi[0][1], hi[1][1]);
+        r.hzm = make_float4(hi[0][2], hi[1][2], mm[0], mm[1]);
+        r.lxy = make_float4(lo[0][0], lo[1][0], lo[0][1], lo[1][1]);
+        r.lzi = make_float4(lo[0][2], lo[1][2], __int_as_float(id[0]), __int_as_float(id[1]));
+        r.vxy = make_float4(vv[0][0], vv[1][0], vv[0][1], vv[1][1]);
+        r.vz = make_float4(vv[0][2], vv[1][2], 0.f, 0.f);
+        reinterpret_cast<JPairMixed *>(d.jrec)[g0 / 2] = r;
+    }
+}
+
+// Smallest block step: below it t + dt would no longer advance t in FP64
+// for t ~ 1, so steps are floored here instead.
+constexpr double kDtMin = 9.094947017729282e-13;  // 2^-40
+
+__host__ __device__ inline double pow2_floor(double x) {
+    int e;
+    frexp(x, &e);  // x = f 2^e, f in [0.5, 1)
+    return ldexp(1.0, e - 1);
+}
+
+// Hermite corrector (FP64) and the next block step.  mode 1 = start: take
+// the forces as the initial acc/jerk and choose the first step from
+// eta_s |a| / |j|.
+__global__ void ens_correct_kernel(EnsDev d, int mode) {
+    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= d.ntot) return;
+    const int s = d.slot[g];
+    if (s < 0) return;
+    const int c = d.cid[g];
+    const int o = d.off[c];
+    const double tb = d.tblock[c];
+    const size_t k = (size_t)o + s;
+    double a1[3], j1[3];
+    for (int q = 0; q < 3; ++q) {
+        a1[q] = d.acc1[3 * k + q];
+        j1[q] = d.jerk1[3 * k + q];
+    }
+    const int N = d.ntot;
+    if (mode == 1) {
+        double an = 0, jn = 0;
+        for (int q = 0; q < 3; ++q) {
+            d.a[q * N + g] = a1[q];
+            d.jk[q * N + g] = j1[q];
+            an += a1[q] * a1[q];
+            jn += j1[q] * j1[q];
+        }
+        double dt0 = (jn > 0) ? d.eta_s * sqrt(an / jn) : d.dt_max;
+        dt0 = fmin(pow2_floor(fmax(dt0, kDtMin)), d.dt_max);
+        d.dt[g] = dt0;
+        return;
+    }
+    const double h = tb - d.t[g];
+    double xp[3], vp[3];
+    predict_state(d, g, tb, xp, vp);
+    double a2e[3], a3[3];
+    const double h2 = h * h, h3 = h2 * h;
+    double sa1 = 0, sj1 = 0, sa2 = 0, sa3 = 0;
+    for (int q = 0; q < 3; ++q) {
+        const double a0 = d.a[q * N + g], j0 = d.jk[q * N + g];
+        const double sn = (-6.0 * (a0 - a1[q]) - h * (4.0 * j0 + 2.0 * j1[q])) / h2;
+        const double cr = (12.0 * (a0 - a1[q]) + 6.0 * h * (j0 + j1[q])) / h3;
+        d.x[q * N + g] = xp[q] + h2 * h2 * (sn / 24.0 + h * cr / 120.0);
+        d.v[q * N + g] = vp[q] + h3 * (sn / 6.0 + h * cr / 24.0);
+        d.a[q * N + g] = a1[q];
+        d.jk[q * N + g] = j1[q];
+        a2e[q] = sn + h * cr;
+        a3[q] = cr;
+        sa1 += a1[q] * a1[q];
+        sj1 += j1[q] * j1[q];
+        sa2 += a2e[q] * a2e[q];
+        sa3 += a3[q] * a3[q];
+    }
+    const double na1 = sqrt(sa1), nj1 = sqrt(sj1), na2 = sqrt(sa2), na3 = sqrt(sa3);
+    const double den = nj1 * na3 + sa2;
+    double dtn = den > 0 ? sqrt(d.eta * (na1 * na2 + sj1) / den) : 2.0 * h;
+    dtn = pow2_floor(fmax(dtn, kDtMin));
+    dtn = fmin(dtn, fmin(2.0 * h, d.dt_max));
+    while (dtn > kDtMin && (fmod(tb, dtn) != 0.0 || (tb < d.t_end && tb + dtn > d.t_end))) dtn *= 0.5;
+    d.t[g] = tb;
+    d.dt[g] = fmax(dtn, kDtMin);
+}
+
+// Before a run: no step may jump over t_end, so every particle lands on it
+// (t_end is a dyadic time and halving keeps t a multiple of dt).
+__global__ void ens_cap_kernel(EnsDev d) {
+    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= d.ntot || d.cid[g] < 0 || g - d.off[d.cid[g]] >= d.n[d.cid[g]]) return;
+    double dt = d.dt[g];
+    while (dt > kDtMin && d.t[g] < d.t_end && d.t[g] + dt > d.t_end) dt *= 0.5;
+    d.dt[g] = dt;
+}
+
+// Kinetic and potential energy of every cluster (FP64, fixed reduction
+// order); pot1 holds the potentials of a mode-1 sweep.
+__global__ void __launch_bounds__(256) ens_energy_kernel(EnsDev d, double *out) {
+    __shared__ double sk[256], sp[256];
+    const int c = blockIdx.x, tid = threadIdx.x;
+    const int n = d.n[c], o = d.off[c], N = d.ntot;
+    double ek = 0, ep = 0;
+    for (int i = tid; i < n; i += 256) {
+        const int g = o + i;
+        const int s = d.slot[g];
+        double v2 = 0;
+        for (int q = 0; q < 3; ++q) v2 += d.v[q * N + g] * d.v[q * N + g];
+        ek += 0.5 * d.m[g] * v2;
+        if (s >= 0) ep += 0.5 * d.m[g] * d.pot1[o + s];
+    }
+    sk[tid] = ek;
+    sp[tid] = ep;
+    __syncthreads();
+    for (int w = 128; w > 0; w >>= 1) {
+        if (tid < w) {
+            sk[tid] += sk[tid + w];
+            sp[tid] += sp[tid + w];
+        }
+        __syncthreads();
+    }
+    if (tid == 0) {
+        out[2 * c] = sk[0];
+        out[2 * c + 1] = sp[0];
+    }
+}
+
+// ---------------------------------------------------------------------------
+
+struct EnsembleStats {
+    double seconds = 0;
+    long long interactions = 0;
+    long long iterations = 0;
+    long long launches = 0;
+    double tuned_h = 0;
+};
+
+class Ensemble {
+  public:
+    Ensemble(int nc, const int *n, const double *eps2, double eta, int mode, int device)
+        : nc_(nc), n_(n, n + nc), eps2_(eps2, eps2 + nc), eta_(eta), mode_(mode), device_(device) {}
+    ~Ensemble() { release(); }
+
+    std::string err;
+
+    int setup();
+    int set_cluster(int c, const double *m, const double (*x)[3], const double (*v)[3]);
+    int start();                                    // forces and first steps at t = 0
+    int run_batched(double t_end, EnsembleStats *st, int tune);
+    int run_per_cluster(double t_end, EnsembleStats *st);
+    int energies(double *ek_ep);                    // [2 nc], all clusters at equal time
+    int get_cluster(int c, double *m, double (*x)[3], double (*v)[3], double (*acc)[3], double (*jerk)[3],
+                    double *t, double *dt);
+
+  private:
+    int fail(const char *what, cudaError_t e) {
+        err = std::string("ensemble: ") + what + ": " + cudaGetErrorString(e);
+        return -1;
+    }
+    void release();
+    int iteration(int mode);  // schedule -> scan -> predict -> force -> correct
+    int sync_host_state();
+    int push_host_state();
+
+    int nc_;
+    std::vector<int> n_;
+    std::vector<double> eps2_;
+    double eta_;
+    int mode_, device_;
+    int kmode_ = kKernMixedP;
+    int ntot_ = 0;
+    long long max_iters_ = 2000000;  // run guards (G6B200_ENS_MAX_ITERS / _SECONDS)
+    double max_seconds_ = 600.0;
+    std::vector<int> off_;
+    std::vector<double> hm_, hx_, hv_;  // host copies of the initial state
+    EnsDev d_{};
+    cudaStream_t stream_ = nullptr;
+    cudaGraphExec_t graph_ = nullptr;
+    int graph_iters_ = 0;
+    int ctas_ = 0, num_sms_ = 148;
+    void *blob_ = nullptr;
+    std::vector<void *> allocs_;
+    // host state for the per-cluster baseline: x,v,a,jk [3][ntot] + t, dt, m
+    std::vector<double> sx_, sv_, sa_, sj_, st_, sdt_, sm_;
+};
+
+void Ensemble::release() {
+    if (graph_) cudaGraphExecDestroy(graph_);
+    graph_ = nullptr;
+    for (void *p : allocs_) cudaFree(p);
+    allocs_.clear();
+    if (stream_) cudaStreamDestroy(stream_);
+    stream_ = nullptr;
+}
+
+#define ECHK(call, what)                              \
+    do {                                              \
+        cudaError_t e_ = (call);                      \
+        if (e_ != cudaSuccess) return fail(what, e_); \
+    } while (0)
+
+int Ensemble::setup() {
+    if (const char *e = getenv("G6B200_ENS_MAX_ITERS")) max_iters_ = atoll(e);
+    if (const char *e = getenv("G6B200_ENS_MAX_SECONDS")) max_seconds_ = atof(e);
+    ECHK(cudaSetDevice(device_), "device");
+    ECHK(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "stream");
+    ECHK(cudaDeviceGetAttribute(&num_sms_, cudaDevAttrMultiProcessorCount, device_), "attr");
+    kmode_ = mode_ == kModeF64 ? kKernF64 : kKernMixedP;
+    off_.assign(nc_ + 1, 0);
+    for (int c = 0; c < nc_; ++c) off_[c + 1] = off_[c] + (n_[c] + 255) / 256 * 256;
+    ntot_ = off_[nc_];
+    std::vector<int> cid(ntot_, -1);
+    std::vector<long long> poff(nc_);
+    long long ptot = 0;
+    for (int c = 0; c < nc_; ++c) {
+        for (int g = off_[c]; g < off_[c + 1]; ++g) cid[g] = c;
+        poff[c] = ptot;
+        const int nj_pad = (n_[c] + tile_of(kmode_) - 1) / tile_of(kmode_) * tile_of(kmode_);
+        ptot += (long long)n_[c] * batch_max_split(kmode_, nj_pad);
+    }
+    auto alloc = [&](void **p, size_t bytes) -> cudaError_t {
+        cudaError_t e = cudaMalloc(p, bytes > 0 ? bytes : 16);
+        if (e == cudaSuccess) {
+            allocs_.push_back(*p);
+            cudaMemsetAsync(*p, 0, bytes > 0 ? bytes : 16, stream_);
+        }
+        return e;
+    };
+    const size_t N = ntot_;
+    void *p;
+    ECHK(alloc(&p, sizeof(int) * (nc_ + 1)), "alloc"); d_.off = (int *)p;
+    ECHK(alloc(&p, sizeof(int) * nc_), "alloc"); d_.n = (int *)p;
+    ECHK(alloc(&p, sizeof(int) * N), "alloc"); d_.cid = (int *)p;
+    ECHK(alloc(&p, sizeof(double) * nc_), "alloc"); d_.eps2 = (double *)p;
+    ECHK(alloc(&p, sizeof(FixedScale) * nc_), "alloc"); d_.fs = (FixedScale *)p;
+    ECHK(alloc(&p, sizeof(long long) * nc_), "alloc"); d_.part_off = (long long *)p;
+    ECHK(alloc(&p, sizeof(double) * 3 * N), "alloc"); d_.x = (double *)p;
+    ECHK(alloc(&p, sizeof(double) * 3 * N), "alloc"); d_.v = (double *)p;
+    ECHK(alloc(&p, sizeof(double) * 3 * N), "alloc"); d_.a = (double *)p;
+    ECHK(alloc(&p, sizeof(double) * 3 * N), "alloc"); d_.jk = (double *)p;
+    ECHK(alloc(&p, sizeof(double) * N), "alloc"); d_.t = (double *)p;
+    ECHK(alloc(&p, sizeof(double) * N), "alloc"); d_.dt = (double *)p;
+    ECHK(alloc(&p, sizeof(double) * N), "alloc"); d_.m = (double *)p;
+    ECHK(alloc(&p, sizeof(int) * N), "alloc"); d_.slot = (int *)p;
+    ECHK(alloc(&p, sizeof(double) * nc_), "alloc"); d_.tblock = (double *)p;
+    ECHK(alloc(&p, sizeof(int) * nc_), "alloc"); d_.count = (int *)p;
+    ECHK(alloc(&p, sizeof(int) * nc_), "alloc"); d_.ntask = (int *)p;
+    ECHK(alloc(&p, sizeof(JRecF64) * N), "alloc"); d_.jrec = p;
+    ECHK(alloc(&p, sizeof(IRec) * N), "alloc"); d_.irec = (IRec *)p;
+    ECHK(alloc(&p, sizeof(double) * 3 * N), "alloc"); d_.acc1 = (double *)p;
+    ECHK(alloc(&p, sizeof(double) * 3 * N), "alloc"); d_.jerk1 = (double *)p;
+    ECHK(alloc(&p, sizeof(double) * N), "alloc"); d_.pot1 = (double *)p;
+    ECHK(alloc(&p, sizeof(int) * N), "alloc"); d_.nn1 = (int *)p;
+    ECHK(alloc(&p, sizeof(Partial) * (size_t)ptot), "alloc"); d_.part = (Partial *)p;
+    ECHK(alloc(&p, sizeof(ForceParams) * nc_), "alloc"); d_.items = (ForceParams *)p;
+    ECHK(alloc(&p, sizeof(int) * (nc_ + 1)), "alloc"); d_.task0 = (int *)p;
+    ECHK(alloc(&p, sizeof(int) * (nc_ + 1)), "alloc"); d_.ipre = (int *)p;
+    ECHK(alloc(&p, sizeof(int) * 4), "alloc"); d_.counter = (int *)p;
+    ECHK(alloc(&p, sizeof(unsigned) * 4), "alloc"); d_.status = (unsigned *)p;
+    ECHK(alloc(&p, sizeof(int) * 4), "alloc"); d_.active = (int *)p;
+    ECHK(alloc(&p, sizeof(unsigned long long) * 2), "alloc"); d_.interactions = (unsigned long long *)p;
+    d_.nc = nc_;
+    d_.ntot = ntot_;
+    d_.eta = eta_;
+    d_.eta_s = 0.01;
+    d_.dt_max = 1.0 / 16;
+    d_.kmode = kmode_;
+    d_.cfg = batch_config(kmode_);
+    ctas_ = batch_ctas(kmode_, d_.cfg, num_sms_);
+    ECHK(cudaMemcpyAsync((void *)d_.off, off_.data(), sizeof(int) * (nc_ + 1), cudaMemcpyHostToDevice, stream_), "copy");
+    ECHK(cudaMemcpyAsync((void *)d_.n, n_.data(), sizeof(int) * nc_, cudaMemcpyHostToDevice, stream_), "copy");
+    ECHK(cudaMemcpyAsync((void *)d_.cid, cid.data(), sizeof(int) * N, cudaMemcpyHostToDevice, stream_), "copy");
+    ECHK(cudaMemcpyAsync((void *)d_.eps2, eps2_.data(), sizeof(double) * nc_, cudaMemcpyHostToDevice, stream_), "copy");
+    ECHK(cudaMemcpyAsync((void *)d_.part_off, poff.data(), sizeof(long long) * nc_, cudaMemcpyHostToDevice, stream_),
+         "copy");
+    hm_.assign(N, 0.0);
+    hx_.assign(3 * N, 0.0);
+    hv_.assign(3 * N, 0.0);
+    ECHK(cudaStreamSynchronize(stream_), "sync");
+    return 0;
+}
+
+int Ensemble::set_cluster(int c, const double *m, const double (*x)[3], const double (*v)[3]) {
+    if (c < 0 || c >= nc_) {
+        err = "ensemble: cluster index out of range";
+        return -1;
+    }
+    const int o = off_[c], N = ntot_;
+    for (int i = 0; i < n_[c]; ++i) {
+        hm_[o + i] = m[i];
+        for (int q = 0; q < 3; ++q) {
+            hx_[q * N + o + i] = x[i][q];
+            hv_[q * N + o + i] = v[i][q];
+        }
+    }
+    return 0;
+}
+
+int Ensemble::push_host_state() {
+    const size_t N = ntot_;
+    ECHK(cudaMemcpyAsync(d_.m, hm_.data(), sizeof(double) * N, cudaMemcpyHostToDevice, stream_), "copy");
+    ECHK(cudaMemcpyAsync(d_.x, hx_.data(), sizeof(double) * 3 * N, cudaMemcpyHostToDevice, stream_), "copy");
+    ECHK(cudaMemcpyAsync(d_.v, hv_.data(), sizeof(double) * 3 * N, cudaMemcpyHostToDevice, stream_), "copy");
+    ECHK(cudaMemsetAsync(d_.t, 0, sizeof(double) * N, stream_), "memset");
+    ECHK(cudaMemsetAsync(d_.a, 0, sizeof(double) * 3 * N, stream_), "memset");
+    ECHK(cudaMemsetAsync(d_.jk, 0, sizeof(double) * 3 * N, stream_), "memset");
+    // fixed-point range per cluster: |x| < 2^(E-2), margin 4 for the motion
+    std::vector<FixedScale> fs(nc_);
+    for (int c = 0; c < nc_; ++c) {
+        double xm = 0;
+        for (int q = 0; q < 3; ++q)
+            for (int i = 0; i < n_[c]; ++i) xm = std::max(xm, std::fabs(hx_[q * N + off_[c] + i]));
+        const int E = xm > 0 ? std::ilogb(xm) + 3 : 1;
+        fs[c].to_units = std::ldexp(1.0, 23 - E);
+        fs[c].hi_unit = std::ldexp(1.0, E - 23);
+        fs[c].lo_unit = std::ldexp(1.0, E - 46);
+    }
+    ECHK(cudaMemcpyAsync((void *)d_.fs, fs.data(), sizeof(FixedScale) * nc_, cudaMemcpyHostToDevice, stream_), "copy");
+    ECHK(cudaStreamSynchronize(stream_), "sync");
+    return 0;
+}
+
+int Ensemble::iteration(int mode) {
+    ens_schedule_kernel<<<nc_, 256, 0, stream_>>>(d_, mode);
+    ens_scan_kernel<<<1, 32, 0, stream_>>>(d_);
+    const int per = kmode_ == kKernMixedP ? 2 : 1;
+    const int units = (ntot_ / per + 255) / 256;
+    ens_predict_kernel<<<units, 256, 0, stream_>>>(d_);
+    BatchArgs ba;
+    ba.items = d_.items;
+    ba.task0 = d_.task0;
+    ba.ipre = d_.ipre;
+    ba.n_items = nc_;
+    ba.H = d_.cfg.H;
+    ba.counter = d_.counter;
+    cudaError_t e = launch_force_batch(stream_, kmode_, d_.cfg, ba, ctas_, ntot_, false, true);
+    if (e != cudaSuccess) return fail("force launch", e);
+    if (mode != 2) ens_correct_kernel<<<(ntot_ + 255) / 256, 256, 0, stream_>>>(d_, mode);
+    return cudaGetLastError() == cudaSuccess ? 0 : -1;
+}
+
+int Ensemble::start() {
+    if (push_host_state()) return -1;
+    if (iteration(1)) return -1;
+    ECHK(cudaStreamSynchronize(stream_), "start");
+    unsigned long long z = 0;
+    ECHK(cudaMemcpy(d_.interactions, &z, sizeof z, cudaMemcpyHostToDevice), "copy");
+    return 0;
+}
+
+int Ensemble::run_batched(double t_end, EnsembleStats *st, int tune) {
+    ECHK(cudaSetDevice(device_), "device");
+    d_.t_end = t_end;
+    if (graph_) {
+        cudaGraphExecDestroy(graph_);
+        graph_ = nullptr;
+    }
+    unsigned long long i0 = 0;
+    ECHK(cudaMemcpy(&i0, d_.interactions, sizeof i0, cudaMemcpyDeviceToHost), "copy");
+    ens_cap_kernel<<<(ntot_ + 255) / 256, 256, 0, stream_>>>(d_);
+    ECHK(cudaStreamSynchronize(stream_), "cap");
+    auto t0 = std::chrono::steady_clock::now();
+    long long iters = 0;
+    // Autotune the i-tile (H warps per j-tile) on the first iterations.
+    if (tune) {
+        const int cands[4] = {8, 4, 2, 1};
+        double best = 1e30;
+        int bestH = d_.cfg.H;
+        cudaEvent_t e0, e1;
+        cudaEventCreate(&e0);
+        cudaEventCreate(&e1);
+        for (int h : cands) {
+            d_.cfg.H = h;
+            ctas_ = batch_ctas(kmode_, d_.cfg, num_sms_);
+            cudaEventRecord(e0, stream_);
+            for (int k = 0; k < 16; ++k)
+                if (iteration(0)) return -1;
+            cudaEventRecord(e1, stream_);
+            cudaEventSynchronize(e1);
+            iters += 16;
+            float ms = 0;
+            cudaEventElapsedTime(&ms, e0, e1);
+            if (ms < best) {
+                best = ms;
+                bestH = h;
+            }
+        }
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        d_.cfg.H = bestH;
+        ctas_ = batch_ctas(kmode_, d_.cfg, num_sms_);
+    }
+    if (st) st->tuned_h = d_.cfg.H;
+    // Capture K iterations as one graph.
+    const int K = 8;
+    cudaGraph_t g;
+    ECHK(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal), "capture");
+    for (int k = 0; k < K; ++k) iteration(0);
+    ECHK(cudaStreamEndCapture(stream_, &g), "capture");
+    ECHK(cudaGraphInstantiate(&graph_, g, 0), "instantiate");
+    cudaGraphDestroy(g);
+    int *h_active = nullptr;
+    ECHK(cudaMallocHost(&h_active, sizeof(int)), "pinned");
+    long long launches = 0;
+    for (;;) {
+        ECHK(cudaGraphLaunch(graph_, stream_), "graph launch");
+        launches += K * 6;
+        iters += K;
+        cudaMemcpyAsync(h_active, d_.active, sizeof(int), cudaMemcpyDeviceToHost, stream_);
+        ECHK(cudaStreamSynchronize(stream_), "run");
+        if (*h_active == 0) break;
+        if (iters > max_iters_ ||
+            std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count() > max_seconds_) {
+            err = "ensemble: iteration or time limit reached";
+            cudaFreeHost(h_active);
+            return -1;
+        }
+    }
+    cudaFreeHost(h_active);
+    auto t1 = std::chrono::steady_clock::now();
+    unsigned long long i1 = 0;
+    unsigned status = 0;
+    ECHK(cudaMemcpy(&i1, d_.interactions, sizeof i1, cudaMemcpyDeviceToHost), "copy");
+    ECHK(cudaMemcpy(&status, d_.status, sizeof status, cudaMemcpyDeviceToHost), "copy");
+    if (status) {
+        err = "ensemble: device status " + std::to_string(status) + " (fixed-point range or copy timeout)";
+        return -2;
+    }
+    if (st) {
+        st->seconds = std::chrono::duration<double>(t1 - t0).count();
+        st->interactions = (long long)(i1 - i0);
+        st->iterations = iters;
+        st->launches = launches;
+    }
+    return 0;
+}
+
+int Ensemble::sync_host_state() {
+    const size_t N = ntot_;
+    sx_.resize(3 * N); sv_.resize(3 * N); sa_.resize(3 * N); sj_.resize(3 * N);
+    st_.resize(N); sdt_.resize(N); sm_.resize(N);
+    ECHK(cudaMemcpy(sx_.data(), d_.x, sizeof(double) * 3 * N, cudaMemcpyDeviceToHost), "copy");
+    ECHK(cudaMemcpy(sv_.data(), d_.v, sizeof(double) * 3 * N, cudaMemcpyDeviceToHost), "copy");
+    ECHK(cudaMemcpy(sa_.data(), d_.a, sizeof(double) * 3 * N, cudaMemcpyDeviceToHost), "copy");
+    ECHK(cudaMemcpy(sj_.data(), d_.jk, sizeof(double) * 3 * N, cudaMemcpyDeviceToHost), "copy");
+    ECHK(cudaMemcpy(st_.data(), d_.t, sizeof(double) * N, cudaMemcpyDeviceToHost), "copy");
+    ECHK(cudaMemcpy(sdt_.data(), d_.dt, sizeof(double) * N, cudaMemcpyDeviceToHost), "copy");
+    ECHK(cudaMemcpy(sm_.data(), d_.m, sizeof(double) * N, cudaMemcpyDeviceToHost), "copy");
+    return 0;
+}
+
+// The plain engine: one g6 engine instance per cluster, one
+// firsthalf/lasthalf call per cluster per block, host-side prediction and
+// correction (kira's own pattern), clusters taking turns.
+int Ensemble::run_per_cluster(double t_end, EnsembleStats *st) {
+    if (sync_host_state()) return -1;
+    const int N = ntot_;
+    for (int g = 0; g < N; ++g)
+        while (sdt_[g] > kDtMin && st_[g] < t_end && st_[g] + sdt_[g] > t_end) sdt_[g] *= 0.5;
+    std::vector<Engine *> eng(nc_, nullptr);
+    int maxn = 0;
+    for (int c = 0; c < nc_; ++c) maxn = std::max(maxn, n_[c]);
+    for (int c = 0; c < nc_; ++c) {
+        Engine *e = new Engine(100000 + c);
+        eng[c] = e;
+        if (e->open(device_, n_[c]) || e->set_mode(mode_) || e->set_npipes(maxn)) {
+            err = "ensemble baseline: " + e->last_error;
+            for (Engine *x : eng) delete x;
+            return -1;
+        }
+        const int o = off_[c];
+        for (int i = 0; i < n_[c]; ++i) {
+            const int g = o + i;
+            double xx[3], vv[3], a2[3], j6[3];
+            for (int q = 0; q < 3; ++q) {
+                xx[q] = sx_[q * N + g];
+                vv[q] = sv_[q * N + g];
+                a2[q] = 0.5 * sa_[q * N + g];
+                j6[q] = sj_[q * N + g] / 6.0;
+            }
+            e->set_j(i, i, st_[g], sm_[g], nullptr, j6, a2, vv, xx);
+        }
+    }
+    std::vector<int> idx(maxn);
+    std::vector<double> xi(3 * (size_t)maxn), vi(3 * (size_t)maxn), acc(3 * (size_t)maxn), jerk(3 * (size_t)maxn),
+        pot(maxn);
+    std::vector<int> nn(maxn);
+    long long inter = 0, iters = 0, launches0 = 0;
+    for (Engine *e : eng) launches0 += e->stats().launches;
+    auto t0 = std::chrono::steady_clock::now();
+    std::vector<char> done(nc_, 0);
+    int active = nc_;
+    int rc = 0;
+    while (active > 0 && rc == 0) {
+        ++iters;
+        if (iters > max_iters_ ||
+            std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count() > max_seconds_) {
+            err = "ensemble baseline: iteration or time limit reached";
+            rc = -1;
+            break;
+        }
+        for (int c = 0; c < nc_ && rc == 0; ++c) {
+            if (done[c]) continue;
+            const int o = off_[c], n = n_[c];
+            double tb = DBL_MAX;
+            for (int i = 0; i < n; ++i) tb = std::min(tb, st_[o + i] + sdt_[o + i]);
+            if (tb > t_end) {
+                done[c] = 1;
+                --active;
+                continue;
+            }
+            int ni = 0;
+            for (int i = 0; i < n; ++i) {
+                const int g = o + i;
+                if (st_[g] + sdt_[g] != tb) continue;
+                const double h = tb - st_[g];
+                for (int q = 0; q < 3; ++q) {
+                    const double a2 = 0.5 * sa_[q * N + g], j6 = sj_[q * N + g] * (1.0 / 6.0);
+                    xi[3 * ni + q] = sx_[q * N + g] + h * (sv_[q * N + g] + h * (a2 + h * j6));
+                    vi[3 * ni + q] = sv_[q * N + g] + h * (2.0 * a2 + h * (3.0 * j6));
+                }
+                idx[ni++] = i;
+            }
+            Engine *e = eng[c];
+            e->set_ti(tb);
+            if (e->firsthalf(n, ni, idx.data(), (const double(*)[3])xi.data(), (const double(*)[3])vi.data(),
+                             eps2_[c], nullptr) ||
+                e->lasthalf(ni, (double(*)[3])acc.data(), (double(*)[3])jerk.data(), pot.data(), nn.data())) {
+                err = "ensemble baseline: " + e->last_error;
+                rc = -1;
+                break;
+            }
+            inter += (long long)ni * n;
+            for (int k = 0; k < ni; ++k) {
+                const int g = o + idx[k];
+                const double h = tb - st_[g], h2 = h * h, h3 = h2 * h;
+                double sa1 = 0, sj1 = 0, sa2 = 0, sa3 = 0;
+                double xn[3], vn[3], a2h[3], j6h[3];
+                for (int q = 0; q < 3; ++q) {
+                    const double a0 = sa_[q * N + g], j0 = sj_[q * N + g];
+                    const double a1 = acc[3 * k + q], j1 = jerk[3 * k + q];
+                    const double sn = (-6.0 * (a0 - a1) - h * (4.0 * j0 + 2.0 * j1)) / h2;
+                    const double cr = (12.0 * (a0 - a1) + 6.0 * h * (j0 + j1)) / h3;
+                    xn[q] = xi[3 * k + q] + h2 * h2 * (sn / 24.0 + h * cr / 120.0);
+                    vn[q] = vi[3 * k + q] + h3 * (sn / 6.0 + h * cr / 24.0);
+                    const double a2e = sn + h * cr;
+                    sa1 += a1 * a1;
+                    sj1 += j1 * j1;
+                    sa2 += a2e * a2e;
+                    sa3 += cr * cr;
+                    sx_[q * N + g] = xn[q];
+                    sv_[q * N + g] = vn[q];
+                    sa_[q * N + g] = a1;
+                    sj_[q * N + g] = j1;
+                    a2h[q] = 0.5 * a1;
+                    j6h[q] = j1 / 6.0;
+                }
+                const double den = std::sqrt(sj1) * std::sqrt(sa3) + sa2;
+                double dtn = den > 0 ? std::sqrt(eta_ * (std::sqrt(sa1) * std::sqrt(sa2) + sj1) / den) : 2.0 * h;
+                dtn = pow2_floor(std::max(dtn, kDtMin));
+                dtn = std::min(dtn, std::min(2.0 * h, d_.dt_max));
+                while (dtn > kDtMin && (std::fmod(tb, dtn) != 0.0 || (tb < t_end && tb + dtn > t_end))) dtn *= 0.5;
+                st_[g] = tb;
+                sdt_[g] = std::max(dtn, kDtMin);
+                e->set_j(idx[k], idx[k], tb, sm_[g], nullptr, j6h, a2h, vn, xn);
+            }
+        }
+    }
+    auto t1 = std::chrono::steady_clock::now();
+    long long launches1 = 0;
+    for (Engine *e : eng) {
+        launches1 += e->stats().launches;
+        delete e;
+    }
+    if (rc) return rc;
+    if (st) {
+        st->seconds = std::chrono::duration<double>(t1 - t0).count();
+        st->interactions = inter;
+        st->iterations = iters;
+        st->launches = launches1 - launches0;
+    }
+    // write the state back so energies/get_cluster see the baseline's result
+    ECHK(cudaMemcpy(d_.x, sx_.data(), sizeof(double) * 3 * N, cudaMemcpyHostToDevice), "copy");
+    ECHK(cudaMemcpy(d_.v, sv_.data(), sizeof(double) * 3 * N, cudaMemcpyHostToDevice), "copy");
+    ECHK(cudaMemcpy(d_.a, sa_.data(), sizeof(double) * 3 * N, cudaMemcpyHostToDevice), "copy");
+    ECHK(cudaMemcpy(d_.jk, sj_.data(), sizeof(double) * 3 * N, cudaMemcpyHostToDevice), "copy");
+    ECHK(cudaMemcpy(d_.t, st_.data(), sizeof(double) * N, cudaMemcpyHostToDevice), "copy");
+    ECHK(cudaMemcpy(d_.dt, sdt_.data(), sizeof(double) * N, cudaMemcpyHostToDevice), "copy");
+    return 0;
+}
+
+int Ensemble::energies(double *ek_ep) {
+    ECHK(cudaSetDevice(device_), "device");
+    if (iteration(2)) return -1;  // all particles, no correction: pot1
+    double *d_out = nullptr;
+    ECHK(cudaMalloc(&d_out, sizeof(double) * 2 * nc_), "alloc");
+    ens_energy_kernel<<<nc_, 256, 0, stream_>>>(d_, d_out);
+    cudaError_t e = cudaMemcpyAsync(ek_ep, d_out, sizeof(double) * 2 * nc_, cudaMemcpyDeviceToHost, stream_);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(stream_);
+    cudaFree(d_out);
+    if (e != cudaSuccess) return fail("energies", e);
+    return 0;
+}
+
+int Ensemble::get_cluster(int c, double *m, double (*x)[3], double (*v)[3], double (*acc)[3], double (*jerk)[3],
+                          double *t, double *dt) {
+    if (c < 0 || c >= nc_) {
+        err = "ensemble: cluster index out of range";
+        return -1;
+    }
+    if (sync_host_state()) return -1;
+    const int o = off_[c], N = ntot_;
+    for (int i = 0; i < n_[c]; ++i) {
+        if (m) m[i] = sm_[o + i];
+        for (int q = 0; q < 3; ++q) {
+            if (x) x[i][q] = sx_[q * N + o + i];
+            if (v) v[i][q] = sv_[q * N + o + i];
+            if (acc) acc[i][q] = sa_[q * N + o + i];
+            if (jerk) jerk[i][q] = sj_[q * N + o + i];
+        }
+        if (t) t[i] = st_[o + i];
+        if (dt) dt[i] = sdt_[o + i];
+    }
+    return 0;
+}
+
+}  // namespace g6
+
+// ---------------------------------------------------------------------------
+// C ABI
+#include <mutex>
+namespace g6 {
+void record_error(const std::string &msg);
+}
+#pragma GCC visibility push(default)
+#include "../../include/g6b200.h"
+#pragma GCC visibility pop
+
+struct g6b200_ensemble {
+    g6::Ensemble *e;
+};
+
+extern "C" {
+
+__attribute__((visibility("default"))) g6b200_ensemble *g6b200_ens_create(int nclusters, const int *n,
+                                                                         const double *eps2, double eta,
+                                                                         int precision, int device) {
+    if (nclusters <= 0 || !n || !eps2) return nullptr;
+    for (int c = 0; c < nclusters; ++c)
+        if (n[c] <= 0) return nullptr;
+    auto *e = new g6::Ensemble(nclusters, n, eps2, eta, precision, device);
+    if (e->setup()) {
+        g6::record_error(e->err);
+        delete e;
+        return nullptr;
+    }
+    return new g6b200_ensemble{e};
+}
+
+__attribute__((visibility("default"))) int g6b200_ens_set_cluster(g6b200_ensemble *h, int c, const double *m,
+                                                                  const double (*x)[3], const double (*v)[3]) {
+    int rc = h->e->set_cluster(c, m, x, v);
+    if (rc) g6::record_error(h->e->err);
+    return rc;
+}
+
+__attribute__((visibility("default"))) int g6b200_ens_start(g6b200_ensemble *h) {
+    int rc = h->e->start();
+    if (rc) g6::record_error(h->e->err);
+    return rc;
+}
+
+__attribute__((visibility("default"))) int g6b200_ens_run(g6b200_ensemble *h, double t_end, int per_cluster,
+                                                          int tune, g6b200_ens_stats *out) {
+    g6::EnsembleStats st;
+    int rc = per_cluster ? h->e->run_per_cluster(t_end, &st) : h->e->run_batched(t_end, &st, tune);
+    if (rc) {
+        g6::record_error(h->e->err);
+        return rc;
+    }
+    if (out) {
+        out->seconds = st.seconds;
+        out->interactions = st.interactions;
+        out->iterations = st.iterations;
+        out->launches = st.launches;
+        out->tuned_h = (int)st.tuned_h;
+    }
+    return 0;
+}
+
+__attribute__((visibility("default"))) int g6b200_ens_energies(g6b200_ensemble *h, double *ek_ep) {
+    int rc = h->e->energies(ek_ep);
+    if (rc) g6::record_error(h->e->err);
+    return rc;
+}
+
+__attribute__((visibility("default"))) int g6b200_ens_get_cluster(g6b200_ensemble *h, int c, double *m,
+                                                                  double (*x)[3], double (*v)[3], double (*acc)[3],
+                                                                  double (*jerk)[3], double *t, double *dt) {
+    int rc = h->e->get_cluster(c, m, x, v, acc, jerk, t, dt);
+    if (rc) g6::record_error(h->e->err);
+    return rc;
+}
+
+__attribute__((visibility("default"))) void g6b200_ens_destroy(g6b200_ensemble *h) {
+    if (!h) return;
+    delete h->e;
+    delete h;
+}
+
+}  // extern "C"

@@ -27,6 +27,7 @@
 // paired layout evaluates two j per FP32x2 instruction (add/mul/fma.f32x2),
 // halving the issue slots per interaction.  FP64 mode does the pair
 // arithmetic and the sums in FP64.
+#include <algorithm>
 #include <cfloat>
 #include "common.cuh"
 #include "kernels.h"
@@ -501,8 +502,14 @@ template <int K, int R> struct MinBlocks {
     static constexpr int value = R >= 4 ? 1 : 2;
 };
 
+// One task: the i-tile `itile_idx` of item p against its j-split `split`.
+// Shared memory holds the two mbarriers (initialised by the caller) and the
+// tile ring; `gt` counts the tiles this CTA consumed before (it sets the
+// ring stage and the mbarrier phase, so a persistent CTA can run many
+// tasks back to back).
 template <int K, int IL, int R, bool NB, bool IDENT, int V>
-__global__ void __launch_bounds__(256, MinBlocks<K, R>::value) force_kernel(const ForceParams p) {
+__device__ __forceinline__ void process_task(const ForceParams &p, int itile_idx, int split, unsigned char *smem,
+                                             int &gt) {
     using Tr = Traits<K>;
     using JRec = typename Tr::JRec;
     using State = typename StateOf<K>::type;
@@ -512,7 +519,6 @@ __global__ void __launch_bounds__(256, MinBlocks<K, R>::value) force_kernel(cons
     constexpr int JL = 32 / IL;
     constexpr unsigned kTileBytes = U * sizeof(JRec);
 
-    extern __shared__ __align__(128) unsigned char smem[];
     uint64_t *bars = reinterpret_cast<uint64_t *>(smem);          // [2], never reused
     JRec *tiles = reinterpret_cast<JRec *>(smem + 128);           // [2][U]
     Partial *red = reinterpret_cast<Partial *>(smem + 128);       // epilogue reuse
@@ -525,7 +531,7 @@ __global__ void __launch_bounds__(256, MinBlocks<K, R>::value) force_kernel(cons
     const int il = lane % IL, jl = lane / IL;
     const int itile = G * IL * R;
     const int islot = g * IL * R + il;  // slot of r = 0 inside the i-tile
-    const int i0 = blockIdx.x * itile + islot;
+    const int i0 = itile_idx * itile + islot;
 
     State st[R];
     bool range_ok = true;
@@ -539,33 +545,31 @@ __global__ void __launch_bounds__(256, MinBlocks<K, R>::value) force_kernel(cons
     }
     if (!range_ok) atomicOr(p.status, ST_RANGE);
 
-    const int s = blockIdx.y;
-    const int jb = s * p.jper;
+    const int jb = split * p.jper;
     const int je = min(jb + p.jper, p.nj_pad);
-    const int ntiles = (je - jb) / T;
+    const int ntiles = max(0, (je - jb) / T);
     const JRec *jrec = reinterpret_cast<const JRec *>(p.jrec);
+    const int g0 = gt;
 
-    if (threadIdx.x == 0) {
-        mbar_init(&bars[0], 1);
-        mbar_init(&bars[1], 1);
-        fence_barrier_init();
-    }
+    // The previous task's epilogue may still read the tile area.
     __syncthreads();
     if (threadIdx.x == 0 && ntiles > 0) {
-        mbar_arrive_expect_tx(&bars[0], kTileBytes);
-        bulk_g2s(tiles, jrec + jb / JPU, kTileBytes, &bars[0]);
+        const int b = g0 & 1;
+        mbar_arrive_expect_tx(&bars[b], kTileBytes);
+        bulk_g2s(tiles + b * U, jrec + jb / JPU, kTileBytes, &bars[b]);
     }
 
     const int per = U / (H * JL);
     const int kbase = h * (U / H) + jl;
     bool ok = true;
     for (int t = 0; t < ntiles; ++t) {
-        const int b = t & 1;
+        const int gg = g0 + t;
+        const int b = gg & 1;
         if (threadIdx.x == 0 && t + 1 < ntiles) {
             mbar_arrive_expect_tx(&bars[b ^ 1], kTileBytes);
             bulk_g2s(tiles + (b ^ 1) * U, jrec + (jb + (t + 1) * T) / JPU, kTileBytes, &bars[b ^ 1]);
         }
-        if (ok) ok = mbar_wait_bounded(&bars[b], (t >> 1) & 1, kWaitLimitNs);
+        if (ok) ok = mbar_wait_bounded(&bars[b], (gg >> 1) & 1, kWaitLimitNs);
         const JRec *S = tiles + b * U;
         const int tb = jb + t * T;
         bool chk = true;
@@ -581,6 +585,7 @@ __global__ void __launch_bounds__(256, MinBlocks<K, R>::value) force_kernel(cons
             consume_tile<K, R, JL, false, NB, IDENT, V>(st, S, kbase, per, tb, p);
         __syncthreads();
     }
+    gt = g0 + ntiles;
     if (!ok) atomicOr(p.status, ST_TMA_TIMEOUT);
 
     // ---- epilogue: lanes -> warps -> (output | split partial)
@@ -611,9 +616,75 @@ __global__ void __launch_bounds__(256, MinBlocks<K, R>::value) force_kernel(cons
             if (p.nsplit == 1)
                 write_final(p, i, q[r]);
             else
-                p.part[(size_t)s * p.ni + i] = q[r];
+                p.part[(size_t)split * p.ni + i] = q[r];
         }
     }
+}
+
+__device__ __forceinline__ void init_bars(unsigned char *smem) {
+    if (threadIdx.x == 0) {
+        uint64_t *bars = reinterpret_cast<uint64_t *>(smem);
+        mbar_init(&bars[0], 1);
+        mbar_init(&bars[1], 1);
+        fence_barrier_init();
+    }
+}
+
+// One call: gridDim.x i-tiles x gridDim.y j-splits, one task per CTA.
+template <int K, int IL, int R, bool NB, bool IDENT, int V>
+__global__ void __launch_bounds__(256, MinBlocks<K, R>::value) force_kernel(const ForceParams p) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    init_bars(smem);
+    int gt = 0;
+    process_task<K, IL, R, NB, IDENT, V>(p, blockIdx.x, blockIdx.y, smem, gt);
+}
+
+// Many calls in one persistent launch: items[k] is one call (its own
+// j-memory, i-records, softening, fixed-point scale and outputs); its tasks
+// are n_itiles(k) x nsplit(k), numbered from task0[k].  CTAs take tasks
+// from a global counter until the list is exhausted.
+template <int K, int IL, int R, bool NB, bool IDENT, int V>
+__global__ void __launch_bounds__(256, MinBlocks<K, R>::value) batch_force_kernel(const BatchArgs a) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    __shared__ int s_task;
+    init_bars(smem);
+    const int itile = (blockDim.x >> 5) / a.H * IL * R;
+    const int total = a.task0[a.n_items];
+    int gt = 0;
+    for (;;) {
+        __syncthreads();
+        if (threadIdx.x == 0) s_task = atomicAdd(a.counter, 1);
+        __syncthreads();
+        const int task = s_task;
+        if (task >= total) break;
+        int lo = 0, hi = a.n_items - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (a.task0[mid] <= task) lo = mid; else hi = mid - 1;
+        }
+        const ForceParams p = a.items[lo];
+        const int local = task - a.task0[lo];
+        const int n_itiles = (p.ni + itile - 1) / itile;
+        process_task<K, IL, R, NB, IDENT, V>(p, local % n_itiles, local / n_itiles, smem, gt);
+    }
+}
+
+// Split reduction for every i of every item with nsplit > 1; ipre[k] is the
+// prefix sum of the items' ni.
+__global__ void batch_reduce_kernel(const BatchArgs a) {
+    const int gi = blockIdx.x * blockDim.x + threadIdx.x;
+    if (gi >= a.ipre[a.n_items]) return;
+    int lo = 0, hi = a.n_items - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (a.ipre[mid] <= gi) lo = mid; else hi = mid - 1;
+    }
+    const ForceParams &p = a.items[lo];
+    if (p.nsplit <= 1) return;
+    const int i = gi - a.ipre[lo];
+    Partial q = p.part[i];
+    for (int s = 1; s < p.nsplit; ++s) add_partial(q, p.part[(size_t)s * p.ni + i]);
+    write_final(p, i, q);
 }
 
 __global__ void reduce_partials_kernel(const ForceParams p) {
@@ -708,6 +779,56 @@ ForceConfig choose_config(int kmode, int ni, int nj_pad, int num_sms, bool nb) {
     }
     c.nsplit = best_split;
     return c;
+}
+
+// ---- batched (multi-item persistent) launches
+
+using BatchFn = void (*)(const BatchArgs);
+
+template <int K>
+static BatchFn pick_batch(bool nb, bool ident) {
+    constexpr int V = kVarUnroll4;
+    if (nb) return ident ? batch_force_kernel<K, 32, 1, true, true, V> : batch_force_kernel<K, 32, 1, true, false, V>;
+    return ident ? batch_force_kernel<K, 32, 1, false, true, V> : batch_force_kernel<K, 32, 1, false, false, V>;
+}
+
+static BatchFn pick_batch(int kmode, bool nb, bool ident) {
+    if (kmode == kKernMixedP) return pick_batch<kKernMixedP>(nb, ident);
+    if (kmode == kKernMixedDS) return pick_batch<kKernMixedDS>(nb, ident);
+    return pick_batch<kKernF64>(nb, ident);
+}
+
+ForceConfig batch_config(int kmode) {
+    (void)kmode;
+    ForceConfig c;
+    c.il = 32;
+    c.r = 1;
+    c.warps = kMaxWarps;
+    c.H = 4;
+    c.nsplit = 0;
+    return c;
+}
+
+int batch_ctas(int kmode, const ForceConfig &cfg, int num_sms) {
+    int per_sm = 0;
+    BatchFn fn = pick_batch(kmode, false, true);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, 32 * cfg.warps, smem_bytes(kmode, cfg));
+    if (per_sm < 1) per_sm = 1;
+    return per_sm * num_sms;
+}
+
+cudaError_t launch_force_batch(cudaStream_t s, int kmode, const ForceConfig &cfg, const BatchArgs &a, int ctas,
+                               int total_i, bool nb, bool ident) {
+    if (a.n_items <= 0) return cudaSuccess;
+    BatchFn fn = pick_batch(kmode, nb, ident);
+    fn<<<ctas, 32 * cfg.warps, smem_bytes(kmode, cfg), s>>>(a);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    if (total_i > 0) {
+        batch_reduce_kernel<<<(total_i + 255) / 256, 256, 0, s>>>(a);
+        e = cudaGetLastError();
+    }
+    return e;
 }
 
 cudaError_t launch_force(cudaStream_t s, int kmode, const ForceConfig &cfg, ForceParams p,

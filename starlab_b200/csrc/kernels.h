@@ -58,6 +58,16 @@ struct ForceParams {
     unsigned *status;
 };
 
+// A batch of calls for the persistent multi-item kernel (device pointers).
+struct BatchArgs {
+    const ForceParams *items;  // [n_items], each with jper/nsplit/H filled in
+    const int *task0;          // [n_items + 1] prefix of n_itiles * nsplit
+    const int *ipre;           // [n_items + 1] prefix of ni
+    int n_items;
+    int H;                     // j-subranges per CTA (same for every item)
+    int *counter;              // task counter, zero before the launch
+};
+
 struct ForceConfig {
     int il;       // i-lanes per warp (1, 8, 32)
     int r;        // i per thread (1, 2, 4; 2 and 4 only with il = 32)
@@ -84,6 +94,57 @@ ForceConfig choose_config(int kmode, int ni, int nj_pad, int num_sms, bool nb);
 cudaError_t launch_force(cudaStream_t s, int kmode, const ForceConfig &cfg, ForceParams p,
                          bool ident, bool nb);
 size_t partial_bytes(const ForceConfig &cfg, int ni);
+
+// Batched launches.  batch_plan fills jper/nsplit/H of one item from its own
+// (ni, nj) only -- never from the rest of the batch -- so an item's sums are
+// bit-identical alone and in any mix.  batch_itile is the i-tile of the
+// batched kernel.
+__host__ __device__ inline int batch_itile(const ForceConfig &cfg) { return cfg.warps / cfg.H * cfg.il * cfg.r; }
+
+__host__ __device__ inline int tile_of(int kmode) { return kmode == kKernF64 ? 128 : 256; }
+
+// Split rule of the batched kernel: a constant number of tasks wanted per
+// item (never the batch size), at least 4 tiles per split.
+__host__ __device__ inline void batch_plan(int kmode, const ForceConfig &cfg, ForceParams &item, int &n_tasks) {
+    const int kTargetTasks = 592;
+    const int T = tile_of(kmode);
+    const int ntiles = item.nj_pad / T;
+    const int itile = batch_itile(cfg);
+    const int n_itiles = (item.ni + itile - 1) / itile;
+    item.H = cfg.H;
+    if (item.ni <= 0) {
+        item.nsplit = 1;
+        item.jper = T;
+        n_tasks = 0;
+        return;
+    }
+    if (ntiles <= 0) {
+        item.nsplit = 1;
+        item.jper = T;
+    } else {
+        int sp = (kTargetTasks + n_itiles - 1) / n_itiles;
+        const int cap = (ntiles + 3) / 4;
+        sp = sp < cap ? sp : cap;
+        sp = sp > 1 ? sp : 1;
+        const int per_split_tiles = (ntiles + sp - 1) / sp;
+        item.jper = per_split_tiles * T;
+        item.nsplit = (ntiles + per_split_tiles - 1) / per_split_tiles;
+    }
+    n_tasks = n_itiles * item.nsplit;
+}
+
+// Largest nsplit batch_plan can choose for nj_pad (sizes the partials).
+__host__ __device__ inline int batch_max_split(int kmode, int nj_pad) {
+    const int ntiles = nj_pad / tile_of(kmode);
+    const int cap = (ntiles + 3) / 4;
+    return cap > 1 ? cap : 1;
+}
+ForceConfig batch_config(int kmode);
+// One persistent launch over all tasks (grid = ctas) + the split reduction
+// over total_i i-particles.
+cudaError_t launch_force_batch(cudaStream_t s, int kmode, const ForceConfig &cfg, const BatchArgs &a, int ctas,
+                               int total_i, bool nb, bool ident);
+int batch_ctas(int kmode, const ForceConfig &cfg, int num_sms);
 
 // Neighbour lists: per-i sort + compaction into ascending address order.
 // offsets[ni+1] (exclusive scan of min(count, cap)), out[total].
