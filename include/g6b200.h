@@ -232,6 +232,40 @@ int g6b200_ens_get_cluster(g6b200_ensemble *h, int c, double *m, double (*x)[3],
                            double (*acc)[3], double (*jerk)[3], double *t, double *dt);
 void g6b200_ens_destroy(g6b200_ensemble *h);
 
+/* ---- Force-call server with continuous batching (no counterpart) -----
+ *
+ * Clients on any host threads open clusters (device-resident j-memory,
+ * admitted against an HBM budget: g6b200_srv_open_cluster blocks until the
+ * cluster's footprint fits), load j-particles, then submit force calls -- a
+ * block time, nj and an i-block with predicted positions and velocities, the
+ * content of one g6calc_firsthalf_ -- and wait for acc, jerk, pot and nn (the
+ * outputs of g6calc_lasthalf2_).  A dispatcher thread runs every pending
+ * call (one per cluster at a time) as one persistent launch; calls arriving
+ * meanwhile join the next launch.  A call's results do not depend on which
+ * other calls share its launch (bit-identical alone or mixed).  precision:
+ * G6B200_FP64 or G6B200_MIXED.  No neighbour lists on this path. */
+typedef struct g6b200_server g6b200_server;
+typedef struct {
+    long long batches, requests, interactions, max_batch;
+    double gpu_ms;
+} g6b200_srv_stats_t;
+g6b200_server *g6b200_srv_create(int device, long long hbm_budget_bytes, int precision, int max_batch);
+int g6b200_srv_open_cluster(g6b200_server *h, long long n_cap, double eps2);  /* cluster id or < 0 */
+int g6b200_srv_close_cluster(g6b200_server *h, int cluster);
+/* Load n j-particles at addresses address[k] (NULL: 0..n-1), as
+ * g6_set_j_particle_ (a2 = acc/2, j6 = jerk/6). */
+int g6b200_srv_set_j(g6b200_server *h, int cluster, int n, const int *address, const double *tj,
+                     const double *mass, const double (*j6)[3], const double (*a2)[3],
+                     const double (*v)[3], const double (*x)[3]);
+long long g6b200_srv_submit(g6b200_server *h, int cluster, double ti, int nj, int ni, const int *index,
+                            const double (*xi)[3], const double (*vi)[3]);  /* request id or < 0 */
+/* Block until the request is done; outputs as g6calc_lasthalf2_; latency_s
+ * = time from submit to completion. */
+int g6b200_srv_wait(g6b200_server *h, long long request, double (*acc)[3], double (*jerk)[3], double *pot,
+                    int *nn, double *latency_s);
+int g6b200_srv_stats(g6b200_server *h, g6b200_srv_stats_t *out);
+void g6b200_srv_destroy(g6b200_server *h);
+
 /* Allocation-free force evaluation.  No counterpart in the reference: the
  * GRAPE-6 library owned its board memory, and this entry point exists for
  * callers of this library that cannot call cudaMalloc -- a host program

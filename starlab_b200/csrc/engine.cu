@@ -567,6 +567,51 @@ int Engine::sweep(int nj, int i0, int ni, double eps2, bool copy_out, double (*a
     return 0;
 }
 
+size_t Engine::footprint_bytes() const {
+    return (size_t)cap_ * (sizeof(double) * JF_COUNT + sizeof(int) + kRecMax) +
+           (size_t)stage_cap_ * (sizeof(double) * JF_COUNT + 2 * sizeof(int));
+}
+
+int Engine::prepare_batch_item(int nj, int ni, const double (*xi)[3], ForceParams &item, cudaEvent_t ready,
+                               unsigned *status) {
+    if (!open_ && open(env_int("G6B200_DEVICE", 0), 0)) return -1;
+    G6_CHECK(cudaSetDevice(device_), "cudaSetDevice");
+    const int km = kmode();
+    const int T = tile_size(km);
+    const int nj_pad = round_up(nj, T);
+    if (nj_pad > 0 && ensure_capacity(nj_pad - 1)) return -1;
+    double xm = xmax_;
+    for (int i = 0; i < ni; ++i)
+        for (int c = 0; c < 3; ++c) xm = std::max(xm, std::fabs(xi[i][c]));
+    xmax_ = xm;
+    if (flush_j()) return -1;
+    const int E = std::max(E_, choose_E(xmax_));
+    if (E != E_) {
+        E_ = E;
+        pred_valid_ = false;
+    }
+    const FixedScale fs = scale();
+    if (!pred_valid_ || pred_ti_ != ti_ || pred_nj_ != nj || pred_mode_ != km || pred_E_ != E_) {
+        // a range report of this prediction lands in the batch's status word
+        launch_predict(stream_, km, d_jraw_, d_jindex_, cap_, nj, nj_pad, ti_, fs, d_jrec_, status);
+        G6_CHECK(cudaGetLastError(), "predict launch");
+        stats_.launches++;
+        pred_valid_ = true;
+        pred_ti_ = ti_;
+        pred_nj_ = nj;
+        pred_mode_ = km;
+        pred_E_ = E_;
+    }
+    G6_CHECK(cudaEventRecord(ready, stream_), "event");
+    item.jrec = d_jrec_;
+    item.nj = nj;
+    item.nj_pad = nj_pad;
+    item.fs = fs;
+    stats_.calls++;
+    stats_.interactions += (long long)ni * nj;
+    return 0;
+}
+
 int Engine::read_neighbours() {
     if (!open_) return -1;
     if (!call_nb_) {

@@ -53,6 +53,24 @@ class Engine {
     int read_neighbours();
     int get_neighbours(int pipe, int max_length, int *nblen, int *nbl);
 
+    // For batched launches (server): flush staged j updates, widen the
+    // fixed-point range for xi, predict j to the current ti if stale -- all
+    // on this instance's stream, completion recorded in `ready` -- and fill
+    // the j-side fields of `item` (jrec, nj, nj_pad, fs).  Returns 0.
+    int prepare_batch_item(int nj, int ni, const double (*xi)[3], ForceParams &item, cudaEvent_t ready,
+                           unsigned *status);
+    // After a fixed-point range report: widen the range (x4) for the next call.
+    void widen_range() {
+        E_ += 2;
+        pred_valid_ = false;
+    }
+    // Make this instance's stream wait for an event of another stream.
+    int wait_event(cudaEvent_t e) { return cudaStreamWaitEvent(stream_, e, 0) == cudaSuccess ? 0 : -1; }
+    bool identity_index() const { return n_nonident_ == 0; }
+    int kernel_mode() const { return kmode(); }
+    int device() const { return device_; }
+    size_t footprint_bytes() const;
+
     const EngineStats &stats() const { return stats_; }
     const ForceConfig &last_config() const { return last_cfg_; }
     std::string last_error;

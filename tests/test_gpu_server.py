@@ -1,0 +1,115 @@
+"""The force-call server: continuous batching across clusters.
+
+* a call's results are bit-identical whether it runs alone or batched with
+  calls of other clusters, and match the FP64 oracle within the mixed-mode
+  tolerance;
+* calls from concurrent client threads all complete correctly;
+* admission by HBM footprint: with a budget for two clusters, a third
+  open waits until one is closed.
+"""
+import threading
+import time
+
+import numpy as np
+import pytest
+
+from helpers import rel_err, rel_err_vec, snapshot
+
+pytestmark = pytest.mark.gpu
+
+EPS2 = 1e-6
+
+
+def load(srv, n, seed):
+    m, x, v, a, j = snapshot(n, seed)
+    c = srv.open_cluster(n, EPS2)
+    srv.set_j(c, 0.0, m, j / 6.0, 0.5 * a, v, x)
+    return c, (m, x, v, a, j)
+
+
+def test_alone_equals_mixed_and_matches_oracle(oracle):
+    from starlab_b200.server import Server
+    srv = Server(precision="mixed")
+    ids = [load(srv, n, 40 + k) for k, n in enumerate((3000, 700, 5000, 1500))]
+    ti = 1.0 / 64
+    c0, (m, x, v, a, j) = ids[0]
+    xp, vp = oracle.predict(ti, 0.0, x, v, 0.5 * a, j / 6.0)
+    idx = np.arange(10, 300, dtype=np.int32)
+    alone = srv.wait(srv.submit(c0, ti, len(m), idx, xp[idx], vp[idx]))
+    # the same call again, now together with calls of the other clusters
+    reqs = []
+    for c, (mm, xx, vv, aa, jj) in ids[1:]:
+        xq, vq = oracle.predict(ti, 0.0, xx, vv, 0.5 * aa, jj / 6.0)
+        k = np.arange(0, len(mm), 3, dtype=np.int32)
+        reqs.append((srv.submit(c, ti, len(mm), k, xq[k], vq[k]), c, k, xq, vq, mm))
+    mixed = srv.wait(srv.submit(c0, ti, len(m), idx, xp[idx], vp[idx]))
+    for q in range(4):
+        assert np.array_equal(alone[q], mixed[q])
+    ra, rj, rp, rn, _ = oracle.force(xp, vp, m, idx, xp[idx], vp[idx], EPS2)
+    assert rel_err_vec(alone[0], ra).max() < 1e-6
+    assert rel_err_vec(alone[1], rj).max() < 1e-5
+    assert rel_err(alone[2], rp).max() < 1e-6
+    for rid, c, k, xq, vq, mm in reqs:
+        got = srv.wait(rid)
+        sub = k[::50]
+        ra, rj, rp, rn, _ = oracle.force(xq, vq, mm, sub, xq[sub], vq[sub], EPS2)
+        assert rel_err_vec(got[0][::50], ra).max() < 1e-6
+    st = srv.stats()
+    assert st["requests"] == 2 + len(reqs) and st["batches"] >= 2
+    srv.close()
+
+
+def test_concurrent_clients():
+    from starlab_b200 import G6Engine
+    from starlab_b200.server import Server
+    srv = Server(precision="mixed")
+    nclients, calls = 8, 5
+    data = [load(srv, 1000 + 300 * k, 80 + k) for k in range(nclients)]
+    results = {}
+
+    def client(k):
+        c, (m, x, v, a, j) = data[k]
+        rng = np.random.default_rng(k)
+        out = []
+        for q in range(calls):
+            ni = int(rng.integers(1, len(m)))
+            idx = np.sort(rng.choice(len(m), ni, replace=False)).astype(np.int32)
+            out.append((idx, srv.wait(srv.submit(c, 0.0, len(m), idx, x[idx], v[idx]))))
+        results[k] = out
+
+    th = [threading.Thread(target=client, args=(k,)) for k in range(nclients)]
+    for t in th:
+        t.start()
+    for t in th:
+        t.join(timeout=120)
+    assert len(results) == nclients
+    # every call equals the plain engine's answer for the same inputs
+    for k in range(nclients):
+        c, (m, x, v, a, j) = data[k]
+        eng = G6Engine(cluster_id=5000 + k, precision="mixed", npipes=len(m))
+        eng.set_j_particles(0.0, m, j / 6.0, 0.5 * a, v, x)
+        eng.set_ti(0.0)
+        for idx, got in results[k]:
+            want = eng.force(len(m), idx, x[idx], v[idx], EPS2)
+            assert rel_err_vec(got[0], want[0]).max() < 1e-9
+            assert np.array_equal(got[3], want[3])
+        eng.close()
+    srv.close()
+
+
+def test_admission_by_hbm_footprint():
+    from starlab_b200.server import Server
+    n = 4096
+    foot = (n + 255) // 256 * 256 * (8 * 17 + 4 + 64) + 16384 * (8 * 17 + 8)
+    srv = Server(precision="mixed", hbm_budget=2 * foot + 1000)
+    a = srv.open_cluster(n, EPS2)
+    b = srv.open_cluster(n, EPS2)
+    opened = []
+    t = threading.Thread(target=lambda: opened.append(srv.open_cluster(n, EPS2)))
+    t.start()
+    time.sleep(0.5)
+    assert not opened  # waiting for memory
+    srv.close_cluster(a)
+    t.join(timeout=30)
+    assert len(opened) == 1
+    srv.close()
