@@ -62,6 +62,10 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=None)
     ap.add_argument("--latency-calls", type=int, default=200)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-ensemble", action="store_true")
+    ap.add_argument("--no-served", action="store_true")
+    ap.add_argument("--ensemble-clusters", type=int, default=256)
+    ap.add_argument("--ensemble-t", type=float, default=1.0)
     return ap.parse_args()
 
 
@@ -177,6 +181,71 @@ def make_cluster(n, seed):
     from starlab_b200 import ics
     masses = ics.salpeter_masses(n, seed + 1)
     return ics.plummer(n, seed, masses=masses)
+
+
+def ensemble_section(nc, t_full, seed):
+    """256 independent Plummer clusters, N log-uniform in [256, 16384],
+    eps2 = (4/N)^2, eta = 0.02, mixed precision: the batched engine over one
+    N-body time unit, and batched vs the plain one-call-per-cluster engine on
+    the same slice [0, 1/64]."""
+    from starlab_b200 import ics
+    from starlab_b200.ensemble import Ensemble
+    rng = np.random.default_rng(seed)
+    ns = np.exp(rng.uniform(np.log(256), np.log(16384), nc)).astype(int)
+    cl = [ics.plummer(int(n), seed * 1000 + k) for k, n in enumerate(ns)]
+    eps2 = (4.0 / ns) ** 2
+
+    def make():
+        return Ensemble([c[0] for c in cl], [c[1] for c in cl], [c[2] for c in cl], eps2, eta=0.02,
+                        precision="mixed")
+
+    out = {"clusters": nc, "n_total": int(ns.sum()), "n_range": [256, 16384], "eta": 0.02}
+    e = make()
+    e.start()
+    ek0, ep0 = e.energies()
+    st = e.run(t_full, tune=True)
+    ek, ep = e.energies()
+    de = np.abs((ek + ep) - (ek0 + ep0)) / np.abs(ek0 + ep0)
+    e.close()
+    out["batched_full"] = {"t_end": t_full, "seconds": st["seconds"], "interactions": st["interactions"],
+                           "interactions_per_s": st["interactions"] / st["seconds"],
+                           "iterations": st["iterations"], "tuned_i_tile": 256 // st["tuned_h"],
+                           "dE_over_E_median": float(np.median(de)), "dE_over_E_max": float(de.max())}
+    slice_t = 1.0 / 64
+    for key, per in (("batched_slice", False), ("per_cluster_slice", True)):
+        e = make()
+        e.start()
+        st = e.run(slice_t, per_cluster=per, tune=not per)
+        e.close()
+        out[key] = {"t_end": slice_t, "seconds": st["seconds"], "interactions": st["interactions"],
+                    "interactions_per_s": st["interactions"] / st["seconds"], "iterations": st["iterations"]}
+    out["speedup_vs_per_cluster"] = (out["batched_slice"]["interactions_per_s"]
+                                     / out["per_cluster_slice"]["interactions_per_s"])
+    return out
+
+
+def served_section(seed):
+    """Force calls from 48 clusters (N log-uniform in [512, 65536]) arriving
+    as Poisson(2000/s), ni ~ 1/ni on [1, N]: the batching server vs the plain
+    engine serving the same stream one call at a time."""
+    from starlab_b200 import G6Engine
+    from starlab_b200.server import Server
+    from starlab_b200.stream import make_clusters, make_stream, run_served, run_sequential
+    clusters = make_clusters(48, seed)
+    calls = make_stream(clusters, 2000.0, 3000, seed)
+    srv = Server(precision="mixed")
+    lat, wall, inter = run_served(srv, clusters, calls)
+    st = srv.stats()
+    srv.close()
+    lat2, wall2, inter2 = run_sequential(
+        lambda k, n: G6Engine(cluster_id=3000 + k, precision="mixed", npipes=n), clusters, calls)
+    return {"clusters": len(clusters), "calls": len(calls), "rate_per_s": 2000.0,
+            "served": {"p50_ms": float(np.percentile(lat, 50) * 1e3), "p99_ms": float(np.percentile(lat, 99) * 1e3),
+                       "interactions_per_s": inter / wall, "batches": st["batches"],
+                       "mean_batch": st["requests"] / max(1, st["batches"]), "max_batch": st["max_batch"]},
+            "one_call_at_a_time": {"p50_ms": float(np.percentile(lat2, 50) * 1e3),
+                                   "p99_ms": float(np.percentile(lat2, 99) * 1e3),
+                                   "interactions_per_s": inter2 / wall2}}
 
 
 def cpu_baseline(n, seed, cores):
@@ -375,6 +444,10 @@ def main():
             "gpu_launches": int(launches),
             "clocks": clocks,
         }
+        if dist.world == 1 and not args.no_ensemble:
+            line["ensemble"] = ensemble_section(args.ensemble_clusters, args.ensemble_t, 2024)
+        if dist.world == 1 and not args.no_served:
+            line["served_stream"] = served_section(5)
         if dist.world == 1 and not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(n, seed, os.cpu_count() or 1)
         print(json.dumps(line), flush=True)
