@@ -70,38 +70,7 @@ def parse():
 
 
 # ---------------------------------------------------------------- plumbing
-class Dist:
-    def __init__(self, use_cuda):
-        self.world = int(os.environ.get("WORLD_SIZE", "1"))
-        self.rank = int(os.environ.get("RANK", "0"))
-        self.local = int(os.environ.get("LOCAL_RANK", "0"))
-        self.pg = None
-        self.use_cuda = use_cuda
-        if self.world > 1:
-            import datetime
-            import torch.distributed as dist
-            backend = "nccl" if use_cuda else "gloo"
-            if use_cuda:
-                import torch
-                torch.cuda.set_device(self.local)
-            dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300))
-            self.dist = dist
-
-    def barrier(self):
-        if self.world > 1:
-            self.dist.barrier()
-
-    def max(self, x):
-        if self.world == 1:
-            return float(x)
-        import torch
-        t = torch.tensor([float(x)], dtype=torch.float64, device="cuda" if self.use_cuda else "cpu")
-        self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
-        return float(t.item())
-
-    def close(self):
-        if self.world > 1:
-            self.dist.destroy_process_group()
+from starlab_b200.dist import Dist, cluster_seed, weak_scaling_value  # noqa: E402
 
 
 class ClockSampler:
@@ -162,13 +131,14 @@ def measured_peaks():
 
 
 def traffic_from_profile():
-    """Per-launch DRAM bytes of the force kernel from the committed ncu
-    summary (profiles/force_mixed_n262144.md: 'traffic_bytes_per_launch')."""
-    p = os.path.join(REPO, "profiles", "force_mixed_n262144.md")
+    """DRAM bytes of one full-sweep force launch (the launch `value` times)
+    from the committed ncu summary profiles/force_sweep_traffic_n262144.md
+    ('traffic_bytes_full_sweep_launch: B'); None when not captured."""
+    p = os.path.join(REPO, "profiles", "force_sweep_traffic_n262144.md")
     if not os.path.exists(p):
         return None
     for line in open(p):
-        if line.strip().startswith("traffic_bytes_per_launch:"):
+        if line.strip().startswith("traffic_bytes_full_sweep_launch:"):
             try:
                 return float(line.split(":", 1)[1].split()[0])
             except (ValueError, IndexError):
@@ -323,7 +293,7 @@ def main():
     from starlab_b200 import G6Engine
 
     n = args.n
-    seed = 11 + 97 * dist.rank
+    seed = cluster_seed(11, dist.rank)
     m, x, v = make_cluster(n, seed)
     z = np.zeros((n, 3))
     eng = G6Engine(cluster_id=0, precision="mixed", npipes=n)
@@ -360,7 +330,7 @@ def main():
     launches = eng.stats()["launches"] - l0
     total_ms = dist.max(sum(step_ms))
     interactions = n * (n - 1)
-    value = dist.world * interactions * args.steps / (total_ms * 1e-3)
+    value = weak_scaling_value(dist.world, interactions, args.steps, total_ms)
 
     # ---- e2e through the C ABI with host buffers
     e2e_steps = args.e2e_steps or max(3, args.steps // 2)

@@ -247,7 +247,9 @@ void g6b200_ens_destroy(g6b200_ensemble *h);
 typedef struct g6b200_server g6b200_server;
 typedef struct {
     long long batches, requests, interactions, max_batch;
-    double gpu_ms;
+    double gpu_ms;    /* device time of all batches */
+    double batch_ms;  /* host wall time spent running batches */
+    double queue_ms;  /* summed time calls waited before their batch began */
 } g6b200_srv_stats_t;
 g6b200_server *g6b200_srv_create(int device, long long hbm_budget_bytes, int precision, int max_batch);
 int g6b200_srv_open_cluster(g6b200_server *h, long long n_cap, double eps2);  /* cluster id or < 0 */

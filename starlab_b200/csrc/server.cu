@@ -51,7 +51,9 @@ struct Request {
 
 struct ServerStats {
     long long batches = 0, requests = 0, interactions = 0, max_batch = 0;
-    double gpu_ms = 0;
+    double gpu_ms = 0;      // device time of the batches (events)
+    double batch_ms = 0;    // host wall time inside run_batch
+    double queue_ms = 0;    // summed time calls waited before their batch started
 };
 
 class Server {
@@ -312,6 +314,7 @@ void Server::loop() {
             }
             pending_.assign(keep.begin(), keep.end());
         }
+        const double tb0 = now();
         int rc = run_batch(batch);
         const double t = now();
         {
@@ -320,8 +323,10 @@ void Server::loop() {
                 if (rc) r->rc = rc;
                 r->done = true;
                 r->t_done = t;
+                stats_.queue_ms += (tb0 - r->t_submit) * 1e3;
                 if (clusters_.count(r->cluster)) clusters_[r->cluster]->busy = false;
             }
+            stats_.batch_ms += (t - tb0) * 1e3;
         }
         cv_done_.notify_all();
         cv_work_.notify_one();
@@ -567,6 +572,8 @@ __attribute__((visibility("default"))) int g6b200_srv_stats(g6b200_server *h, g6
     out->interactions = st.interactions;
     out->max_batch = st.max_batch;
     out->gpu_ms = st.gpu_ms;
+    out->batch_ms = st.batch_ms;
+    out->queue_ms = st.queue_ms;
     return 0;
 }
 

@@ -15,7 +15,8 @@ from .g6 import G6Error, load_library, _PREC
 
 class SrvStats(ctypes.Structure):
     _fields_ = [("batches", ctypes.c_longlong), ("requests", ctypes.c_longlong),
-                ("interactions", ctypes.c_longlong), ("max_batch", ctypes.c_longlong), ("gpu_ms", ctypes.c_double)]
+                ("interactions", ctypes.c_longlong), ("max_batch", ctypes.c_longlong), ("gpu_ms", ctypes.c_double),
+                ("batch_ms", ctypes.c_double), ("queue_ms", ctypes.c_double)]
 
 
 def _bind(lib):
