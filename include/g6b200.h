@@ -239,11 +239,16 @@ void g6b200_ens_destroy(g6b200_ensemble *h);
  * cluster's footprint fits), load j-particles, then submit force calls -- a
  * block time, nj and an i-block with predicted positions and velocities, the
  * content of one g6calc_firsthalf_ -- and wait for acc, jerk, pot and nn (the
- * outputs of g6calc_lasthalf2_).  A dispatcher thread runs every pending
- * call (one per cluster at a time) as one persistent launch; calls arriving
- * meanwhile join the next launch.  A call's results do not depend on which
- * other calls share its launch (bit-identical alone or mixed).  precision:
- * G6B200_FP64 or G6B200_MIXED.  No neighbour lists on this path. */
+ * outputs of g6calc_lasthalf2_).  Two dispatcher threads (lanes) run the
+ * pending calls as batched launches: calls with ni*nj up to G6B200_SRV_SMALL
+ * (default 1e8 pair interactions) as one persistent launch on a
+ * high-priority stream, larger calls one CTA per task on a low-priority
+ * stream, so short calls are not held behind long ones; calls arriving while
+ * a launch runs join the next one.  Every call predicts its cluster's
+ * j-set into its own buffer, so calls of one cluster at different block times
+ * may share a launch.  A call's results do not depend on which other calls
+ * share its launch (bit-identical alone or mixed).  precision: G6B200_FP64 or
+ * G6B200_MIXED.  No neighbour lists on this path. */
 typedef struct g6b200_server g6b200_server;
 typedef struct {
     long long batches, requests, interactions, max_batch;

@@ -573,7 +573,7 @@ size_t Engine::footprint_bytes() const {
 }
 
 int Engine::prepare_batch_item(int nj, int ni, const double (*xi)[3], ForceParams &item, cudaEvent_t ready,
-                               unsigned *status) {
+                               unsigned *status, void *dst) {
     if (!open_ && open(env_int("G6B200_DEVICE", 0), 0)) return -1;
     G6_CHECK(cudaSetDevice(device_), "cudaSetDevice");
     const int km = kmode();
@@ -591,7 +591,11 @@ int Engine::prepare_batch_item(int nj, int ni, const double (*xi)[3], ForceParam
         pred_valid_ = false;
     }
     const FixedScale fs = scale();
-    if (!pred_valid_ || pred_ti_ != ti_ || pred_nj_ != nj || pred_mode_ != km || pred_E_ != E_) {
+    if (dst) {
+        launch_predict(stream_, km, d_jraw_, d_jindex_, cap_, nj, nj_pad, ti_, fs, dst, status);
+        G6_CHECK(cudaGetLastError(), "predict launch");
+        stats_.launches++;
+    } else if (!pred_valid_ || pred_ti_ != ti_ || pred_nj_ != nj || pred_mode_ != km || pred_E_ != E_) {
         // a range report of this prediction lands in the batch's status word
         launch_predict(stream_, km, d_jraw_, d_jindex_, cap_, nj, nj_pad, ti_, fs, d_jrec_, status);
         G6_CHECK(cudaGetLastError(), "predict launch");
@@ -603,7 +607,7 @@ int Engine::prepare_batch_item(int nj, int ni, const double (*xi)[3], ForceParam
         pred_E_ = E_;
     }
     G6_CHECK(cudaEventRecord(ready, stream_), "event");
-    item.jrec = d_jrec_;
+    item.jrec = dst ? dst : d_jrec_;
     item.nj = nj;
     item.nj_pad = nj_pad;
     item.fs = fs;

@@ -57,8 +57,12 @@ class Engine {
     // fixed-point range for xi, predict j to the current ti if stale -- all
     // on this instance's stream, completion recorded in `ready` -- and fill
     // the j-side fields of `item` (jrec, nj, nj_pad, fs).  Returns 0.
+    // With dst != nullptr the j-set is predicted into dst (nj_pad records of
+    // this instance's kernel layout), always, and the cached prediction is
+    // left alone -- so calls of one cluster at different block times can
+    // share a launch.
     int prepare_batch_item(int nj, int ni, const double (*xi)[3], ForceParams &item, cudaEvent_t ready,
-                           unsigned *status);
+                           unsigned *status, void *dst = nullptr);
     // After a fixed-point range report: widen the range (x4) for the next call.
     void widen_range() {
         E_ += 2;

@@ -549,6 +549,7 @@ int Ensemble::iteration(int mode) {
     ba.n_items = nc_;
     ba.H = d_.cfg.H;
     ba.counter = d_.counter;
+    ba.one_task_per_cta = 0;
     cudaError_t e = launch_force_batch(stream_, kmode_, d_.cfg, ba, ctas_, ntot_, false, true);
     if (e != cudaSuccess) return fail("force launch", e);
     if (mode != 2) ens_correct_kernel<<<(ntot_ + 255) / 256, 256, 0, stream_>>>(d_, mode);

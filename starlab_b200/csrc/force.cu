@@ -639,10 +639,12 @@ __global__ void __launch_bounds__(256, MinBlocks<K, R>::value) force_kernel(cons
     process_task<K, IL, R, NB, IDENT, V>(p, blockIdx.x, blockIdx.y, smem, gt);
 }
 
-// Many calls in one persistent launch: items[k] is one call (its own
-// j-memory, i-records, softening, fixed-point scale and outputs); its tasks
-// are n_itiles(k) x nsplit(k), numbered from task0[k].  CTAs take tasks
-// from a global counter until the list is exhausted.
+// Many calls in one launch: items[k] is one call (its own j-memory,
+// i-records, softening, fixed-point scale and outputs); its tasks are
+// n_itiles(k) x nsplit(k), numbered from task0[k].  Persistent form: CTAs
+// take tasks from a global counter until the list is exhausted.  With
+// one_task_per_cta, CTA b runs task b (so CTAs of other launches can be
+// scheduled as these retire).
 template <int K, int IL, int R, bool NB, bool IDENT, int V>
 __global__ void __launch_bounds__(256, MinBlocks<K, R>::value) batch_force_kernel(const BatchArgs a) {
     extern __shared__ __align__(128) unsigned char smem[];
@@ -651,9 +653,9 @@ __global__ void __launch_bounds__(256, MinBlocks<K, R>::value) batch_force_kerne
     const int itile = (blockDim.x >> 5) / a.H * IL * R;
     const int total = a.task0[a.n_items];
     int gt = 0;
-    for (;;) {
+    for (int it = 0;; ++it) {
         __syncthreads();
-        if (threadIdx.x == 0) s_task = atomicAdd(a.counter, 1);
+        if (threadIdx.x == 0) s_task = a.one_task_per_cta ? (it == 0 ? (int)blockIdx.x : total) : atomicAdd(a.counter, 1);
         __syncthreads();
         const int task = s_task;
         if (task >= total) break;

@@ -66,6 +66,7 @@ struct BatchArgs {
     int n_items;
     int H;                     // j-subranges per CTA (same for every item)
     int *counter;              // task counter, zero before the launch
+    int one_task_per_cta;      // 1: grid = tasks, CTA b runs task b (no counter)
 };
 
 struct ForceConfig {
@@ -142,6 +143,7 @@ __host__ __device__ inline int batch_max_split(int kmode, int nj_pad) {
 ForceConfig batch_config(int kmode);
 // One persistent launch over all tasks (grid = ctas) + the split reduction
 // over total_i i-particles.
+// ctas: persistent grid size, or (one_task_per_cta) the total task count.
 cudaError_t launch_force_batch(cudaStream_t s, int kmode, const ForceConfig &cfg, const BatchArgs &a, int ctas,
                                int total_i, bool nb, bool ident);
 int batch_ctas(int kmode, const ForceConfig &cfg, int num_sms);

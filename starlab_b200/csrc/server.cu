@@ -19,6 +19,7 @@
 #include <chrono>
 #include <condition_variable>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <deque>
 #include <map>
@@ -37,6 +38,7 @@ void record_error(const std::string &msg);
 struct Request {
     long long id;
     int cluster;
+    int lane;
     double ti, eps2;
     int nj, ni;
     std::vector<int> index;
@@ -47,6 +49,7 @@ struct Request {
     int rc = 0;
     bool done = false;
     double t_submit = 0, t_done = 0;
+    std::condition_variable cv;  // signalled once, when done (waits on the server mutex)
 };
 
 struct ServerStats {
@@ -54,6 +57,31 @@ struct ServerStats {
     double gpu_ms = 0;      // device time of the batches (events)
     double batch_ms = 0;    // host wall time inside run_batch
     double queue_ms = 0;    // summed time calls waited before their batch started
+};
+
+class Server;
+
+// One dispatch lane: its own stream (with a priority), buffers and thread.
+// Lane 0 takes small calls and launches persistently on a high-priority
+// stream; lane 1 takes large calls, one CTA per task on a low-priority
+// stream, so small-call CTAs are scheduled as large-call CTAs retire.
+struct Lane {
+    int id = 0;
+    bool persistent = true;
+    std::deque<std::shared_ptr<Request>> pending;
+    std::thread thread;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev_clear = nullptr, ev_t0 = nullptr, ev_t1 = nullptr;
+    std::vector<cudaEvent_t> ready;  // one per call slot
+    size_t cap_i = 0, cap_part = 0, cap_jrec = 0;
+    int cap_items = 0;
+    IRec *h_irec = nullptr, *d_irec = nullptr;
+    unsigned char *h_out = nullptr, *d_out = nullptr;
+    Partial *d_part = nullptr;
+    unsigned char *d_jrec = nullptr;
+    ForceParams *h_items = nullptr, *d_items = nullptr;
+    int *h_pre = nullptr, *d_pre = nullptr;
+    int *d_counter = nullptr;
 };
 
 class Server {
@@ -84,12 +112,12 @@ class Server {
         std::mutex mu;
         long long footprint = 0;
         double eps2 = 0;
-        bool busy = false;  // a call of this cluster is in the current batch
-        cudaEvent_t ready = nullptr;
+        int inflight = 0;  // calls pending or running
     };
-    void loop();
-    int run_batch(std::vector<std::shared_ptr<Request>> &batch);
-    int ensure(size_t ni_total, size_t parts, int n_items);
+    void loop(Lane &L);
+    int run_batch(Lane &L, std::vector<std::shared_ptr<Request>> &batch);
+    int ensure(Lane &L, size_t ni_total, size_t parts, size_t jrec_bytes, int n_items);
+    void free_lane(Lane &L);
     static double now() {
         return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
     }
@@ -98,27 +126,17 @@ class Server {
     long long budget_, used_ = 0;
     int precision_, max_batch_;
     int kmode_ = kKernMixedP;
+    long long small_max_ = 100000000;  // calls with ni * nj <= this go to lane 0
     std::mutex mu_;
     std::condition_variable cv_work_, cv_done_, cv_mem_;
     std::map<int, std::unique_ptr<Cluster>> clusters_;
     int next_cluster_ = 0;
-    std::deque<std::shared_ptr<Request>> pending_;
     std::map<long long, std::shared_ptr<Request>> inflight_;
     long long next_id_ = 1;
     bool stop_ = false;
-    std::thread thread_;
+    bool started_ = false;
     ServerStats stats_;
-    // device batch buffers
-    cudaStream_t stream_ = nullptr;
-    cudaEvent_t ev_clear_ = nullptr, ev_t0_ = nullptr, ev_t1_ = nullptr;
-    size_t cap_i_ = 0, cap_part_ = 0;
-    int cap_items_ = 0;
-    IRec *h_irec_ = nullptr, *d_irec_ = nullptr;
-    unsigned char *h_out_ = nullptr, *d_out_ = nullptr;  // status + per-request outputs
-    Partial *d_part_ = nullptr;
-    ForceParams *h_items_ = nullptr, *d_items_ = nullptr;
-    int *h_pre_ = nullptr, *d_pre_ = nullptr;  // task0 [n+1] then ipre [n+1]
-    int *d_counter_ = nullptr;
+    Lane lanes_[2];
     int ctas_ = 0;
     ForceConfig cfg_{};
 };
@@ -128,52 +146,61 @@ int Server::start() {
         err = "server: bad device";
         return -1;
     }
+    if (const char *e = getenv("G6B200_SRV_SMALL")) small_max_ = atoll(e);
     kmode_ = precision_ == kModeF64 ? kKernF64 : kKernMixedP;
-    if (cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking) != cudaSuccess ||
-        cudaEventCreateWithFlags(&ev_clear_, cudaEventDisableTiming) != cudaSuccess ||
-        cudaEventCreate(&ev_t0_) != cudaSuccess || cudaEventCreate(&ev_t1_) != cudaSuccess ||
-        cudaMalloc(&d_counter_, 16) != cudaSuccess) {
-        err = "server: CUDA setup failed";
-        return -1;
+    int lo = 0, hi = 0;
+    cudaDeviceGetStreamPriorityRange(&lo, &hi);  // hi = greatest priority (numerically lowest)
+    for (int k = 0; k < 2; ++k) {
+        Lane &L = lanes_[k];
+        L.id = k;
+        L.persistent = k == 0;
+        if (cudaStreamCreateWithPriority(&L.stream, cudaStreamNonBlocking, k == 0 ? hi : lo) != cudaSuccess ||
+            cudaEventCreateWithFlags(&L.ev_clear, cudaEventDisableTiming) != cudaSuccess ||
+            cudaEventCreate(&L.ev_t0) != cudaSuccess || cudaEventCreate(&L.ev_t1) != cudaSuccess ||
+            cudaMalloc(&L.d_counter, 16) != cudaSuccess) {
+            err = "server: CUDA setup failed";
+            return -1;
+        }
     }
     cfg_ = batch_config(kmode_);
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device_);
     ctas_ = batch_ctas(kmode_, cfg_, sms);
-    thread_ = std::thread([this] { loop(); });
+    for (int k = 0; k < 2; ++k) lanes_[k].thread = std::thread([this, k] { loop(lanes_[k]); });
+    started_ = true;
     return 0;
+}
+
+void Server::free_lane(Lane &L) {
+    if (L.h_irec) cudaFreeHost(L.h_irec);
+    if (L.h_out) cudaFreeHost(L.h_out);
+    if (L.h_items) cudaFreeHost(L.h_items);
+    if (L.h_pre) cudaFreeHost(L.h_pre);
+    for (void *p : {(void *)L.d_irec, (void *)L.d_out, (void *)L.d_part, (void *)L.d_items, (void *)L.d_pre,
+                    (void *)L.d_counter, (void *)L.d_jrec})
+        if (p) cudaFree(p);
+    for (cudaEvent_t e : L.ready) cudaEventDestroy(e);
+    L.ready.clear();
+    for (cudaEvent_t e : {L.ev_clear, L.ev_t0, L.ev_t1})
+        if (e) cudaEventDestroy(e);
+    if (L.stream) cudaStreamDestroy(L.stream);
+    L = Lane();
 }
 
 void Server::shutdown() {
     {
         std::lock_guard<std::mutex> lk(mu_);
-        if (stop_ && !thread_.joinable()) return;
+        if (stop_) return;
         stop_ = true;
     }
     cv_work_.notify_all();
-    if (thread_.joinable()) thread_.join();
+    cv_mem_.notify_all();
+    for (Lane &L : lanes_)
+        if (L.thread.joinable()) L.thread.join();
     cudaSetDevice(device_);
-    for (auto &kv : clusters_) {
-        if (kv.second->ready) cudaEventDestroy(kv.second->ready);
-        kv.second->eng.reset();
-    }
+    for (auto &kv : clusters_) kv.second->eng.reset();
     clusters_.clear();
-    if (h_irec_) cudaFreeHost(h_irec_);
-    if (h_out_) cudaFreeHost(h_out_);
-    if (h_items_) cudaFreeHost(h_items_);
-    if (h_pre_) cudaFreeHost(h_pre_);
-    for (void *p : {(void *)d_irec_, (void *)d_out_, (void *)d_part_, (void *)d_items_, (void *)d_pre_,
-                    (void *)d_counter_})
-        if (p) cudaFree(p);
-    h_irec_ = nullptr; h_out_ = nullptr; h_items_ = nullptr; h_pre_ = nullptr;
-    d_irec_ = nullptr; d_out_ = nullptr; d_part_ = nullptr; d_items_ = nullptr; d_pre_ = nullptr;
-    d_counter_ = nullptr;
-    if (ev_clear_) cudaEventDestroy(ev_clear_);
-    if (ev_t0_) cudaEventDestroy(ev_t0_);
-    if (ev_t1_) cudaEventDestroy(ev_t1_);
-    if (stream_) cudaStreamDestroy(stream_);
-    ev_clear_ = ev_t0_ = ev_t1_ = nullptr;
-    stream_ = nullptr;
+    for (Lane &L : lanes_) free_lane(L);
 }
 
 int Server::open_cluster(long long n_cap, double eps2) {
@@ -194,8 +221,7 @@ int Server::open_cluster(long long n_cap, double eps2) {
     cl->eng = std::make_unique<Engine>(200000 + id);
     lk.unlock();
     Engine &e = *cl->eng;
-    if (e.open(device_, (int)n_cap) || e.set_mode(precision_) || e.set_npipes((int)std::max<long long>(n_cap, 1)) ||
-        cudaEventCreateWithFlags(&cl->ready, cudaEventDisableTiming) != cudaSuccess) {
+    if (e.open(device_, (int)n_cap) || e.set_mode(precision_) || e.set_npipes((int)std::max<long long>(n_cap, 1))) {
         err = "server: " + e.last_error;
         lk.lock();
         used_ -= foot;
@@ -213,19 +239,13 @@ int Server::close_cluster(int c) {
         std::unique_lock<std::mutex> lk(mu_);
         auto it = clusters_.find(c);
         if (it == clusters_.end()) return -1;
-        // wait until none of its calls is pending or in flight
-        cv_done_.wait(lk, [&] {
-            if (it->second->busy) return false;
-            for (auto &r : pending_)
-                if (r->cluster == c) return false;
-            return true;
-        });
+        Cluster *p = it->second.get();
+        cv_done_.wait(lk, [&] { return p->inflight == 0; });
         cl = std::move(it->second);
         clusters_.erase(it);
         used_ -= cl->footprint;
     }
     cv_mem_.notify_all();
-    if (cl->ready) cudaEventDestroy(cl->ready);
     cl->eng.reset();
     return 0;
 }
@@ -260,17 +280,19 @@ long long Server::submit(int c, double ti, int nj, int ni, const int *index, con
     r->index.assign(index, index + ni);
     r->xi.assign(&xi[0][0], &xi[0][0] + 3 * (size_t)ni);
     r->vi.assign(&vi[0][0], &vi[0][0] + 3 * (size_t)ni);
+    r->lane = (long long)ni * nj <= small_max_ ? 0 : 1;
     r->t_submit = now();
     {
         std::lock_guard<std::mutex> lk(mu_);
         auto it = clusters_.find(c);
-        if (it == clusters_.end() || ni < 0 || nj <= 0) return -1;
+        if (it == clusters_.end() || ni < 0 || nj <= 0 || stop_) return -1;
         r->eps2 = it->second->eps2;
+        it->second->inflight++;
         r->id = next_id_++;
-        pending_.push_back(r);
+        lanes_[r->lane].pending.push_back(r);
         inflight_[r->id] = r;
     }
-    cv_work_.notify_one();
+    cv_work_.notify_all();
     return r->id;
 }
 
@@ -281,7 +303,7 @@ int Server::wait(long long id, double (*acc)[3], double (*jerk)[3], double *pot,
         auto it = inflight_.find(id);
         if (it == inflight_.end()) return -1;
         r = it->second;
-        cv_done_.wait(lk, [&] { return r->done; });
+        r->cv.wait(lk, [&] { return r->done; });
         inflight_.erase(id);
     }
     if (r->rc) return r->rc;
@@ -294,28 +316,21 @@ int Server::wait(long long id, double (*acc)[3], double (*jerk)[3], double *pot,
     return 0;
 }
 
-void Server::loop() {
+void Server::loop(Lane &L) {
     cudaSetDevice(device_);
     for (;;) {
         std::vector<std::shared_ptr<Request>> batch;
         {
             std::unique_lock<std::mutex> lk(mu_);
-            cv_work_.wait(lk, [&] { return stop_ || !pending_.empty(); });
-            if (stop_ && pending_.empty()) return;
-            std::vector<std::shared_ptr<Request>> keep;
-            for (auto &r : pending_) {
-                Cluster *cl = clusters_.count(r->cluster) ? clusters_[r->cluster].get() : nullptr;
-                if (cl && !cl->busy && (int)batch.size() < max_batch_) {
-                    cl->busy = true;
-                    batch.push_back(r);
-                } else {
-                    keep.push_back(r);
-                }
+            cv_work_.wait(lk, [&] { return stop_ || !L.pending.empty(); });
+            if (stop_ && L.pending.empty()) return;
+            while (!L.pending.empty() && (int)batch.size() < max_batch_) {
+                batch.push_back(L.pending.front());
+                L.pending.pop_front();
             }
-            pending_.assign(keep.begin(), keep.end());
         }
         const double tb0 = now();
-        int rc = run_batch(batch);
+        int rc = run_batch(L, batch);
         const double t = now();
         {
             std::lock_guard<std::mutex> lk(mu_);
@@ -324,65 +339,80 @@ void Server::loop() {
                 r->done = true;
                 r->t_done = t;
                 stats_.queue_ms += (tb0 - r->t_submit) * 1e3;
-                if (clusters_.count(r->cluster)) clusters_[r->cluster]->busy = false;
+                auto it = clusters_.find(r->cluster);
+                if (it != clusters_.end()) it->second->inflight--;
+                r->cv.notify_all();
             }
             stats_.batch_ms += (t - tb0) * 1e3;
         }
-        cv_done_.notify_all();
-        cv_work_.notify_one();
+        cv_done_.notify_all();  // close_cluster waiters
     }
 }
 
-int Server::ensure(size_t ni_total, size_t parts, int n_items) {
-    if (ni_total > cap_i_) {
-        size_t n = std::max(ni_total, cap_i_ * 2);
-        if (h_irec_) cudaFreeHost(h_irec_);
-        if (d_irec_) cudaFree(d_irec_);
-        if (h_out_) cudaFreeHost(h_out_);
-        if (d_out_) cudaFree(d_out_);
-        if (cudaMallocHost(&h_irec_, sizeof(IRec) * n) || cudaMalloc(&d_irec_, sizeof(IRec) * n) ||
-            cudaMallocHost(&h_out_, 16 + 60 * n) || cudaMalloc(&d_out_, 16 + 60 * n))
+int Server::ensure(Lane &L, size_t ni_total, size_t parts, size_t jrec_bytes, int n_items) {
+    if (ni_total > L.cap_i) {
+        size_t n = std::max(ni_total, L.cap_i * 2);
+        if (L.h_irec) cudaFreeHost(L.h_irec);
+        if (L.d_irec) cudaFree(L.d_irec);
+        if (L.h_out) cudaFreeHost(L.h_out);
+        if (L.d_out) cudaFree(L.d_out);
+        if (cudaMallocHost(&L.h_irec, sizeof(IRec) * n) || cudaMalloc(&L.d_irec, sizeof(IRec) * n) ||
+            cudaMallocHost(&L.h_out, 16 + 60 * n) || cudaMalloc(&L.d_out, 16 + 60 * n))
             return -1;
-        cap_i_ = n;
+        L.cap_i = n;
     }
-    if (parts > cap_part_) {
-        size_t n = std::max(parts, cap_part_ * 2);
-        if (d_part_) cudaFree(d_part_);
-        if (cudaMalloc(&d_part_, sizeof(Partial) * n)) return -1;
-        cap_part_ = n;
+    if (parts > L.cap_part) {
+        size_t n = std::max(parts, L.cap_part * 2);
+        if (L.d_part) cudaFree(L.d_part);
+        if (cudaMalloc(&L.d_part, sizeof(Partial) * n)) return -1;
+        L.cap_part = n;
     }
-    if (n_items > cap_items_) {
-        int n = std::max(n_items, cap_items_ * 2);
-        if (h_items_) cudaFreeHost(h_items_);
-        if (d_items_) cudaFree(d_items_);
-        if (h_pre_) cudaFreeHost(h_pre_);
-        if (d_pre_) cudaFree(d_pre_);
-        if (cudaMallocHost(&h_items_, sizeof(ForceParams) * n) || cudaMalloc(&d_items_, sizeof(ForceParams) * n) ||
-            cudaMallocHost(&h_pre_, sizeof(int) * 2 * (n + 1)) || cudaMalloc(&d_pre_, sizeof(int) * 2 * (n + 1)))
+    if (jrec_bytes > L.cap_jrec) {
+        size_t n = std::max(jrec_bytes, L.cap_jrec * 2);
+        if (L.d_jrec) cudaFree(L.d_jrec);
+        if (cudaMalloc(&L.d_jrec, n)) return -1;
+        L.cap_jrec = n;
+    }
+    if (n_items > L.cap_items) {
+        int n = std::max(n_items, L.cap_items * 2);
+        if (L.h_items) cudaFreeHost(L.h_items);
+        if (L.d_items) cudaFree(L.d_items);
+        if (L.h_pre) cudaFreeHost(L.h_pre);
+        if (L.d_pre) cudaFree(L.d_pre);
+        if (cudaMallocHost(&L.h_items, sizeof(ForceParams) * n) || cudaMalloc(&L.d_items, sizeof(ForceParams) * n) ||
+            cudaMallocHost(&L.h_pre, sizeof(int) * 2 * (n + 1)) || cudaMalloc(&L.d_pre, sizeof(int) * 2 * (n + 1)))
             return -1;
-        cap_items_ = n;
+        L.cap_items = n;
+    }
+    while ((int)L.ready.size() < n_items) {
+        cudaEvent_t e;
+        if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming)) return -1;
+        L.ready.push_back(e);
     }
     return 0;
 }
 
-int Server::run_batch(std::vector<std::shared_ptr<Request>> &batch) {
+int Server::run_batch(Lane &L, std::vector<std::shared_ptr<Request>> &batch) {
     const int nb = (int)batch.size();
     if (nb == 0) return 0;
-    size_t ni_total = 0, parts = 0;
+    const int T = tile_of(kmode_);
+    const size_t rec = kmode_ == kKernF64 ? sizeof(JRecF64) : sizeof(JRecMixed);
+    size_t ni_total = 0, parts = 0, jbytes = 0;
     for (auto &r : batch) {
+        const int nj_pad = (r->nj + T - 1) / T * T;
         ni_total += r->ni;
-        const int nj_pad = (r->nj + tile_of(kmode_) - 1) / tile_of(kmode_) * tile_of(kmode_);
         parts += (size_t)r->ni * batch_max_split(kmode_, nj_pad);
+        jbytes += (size_t)nj_pad * rec;
     }
-    if (ensure(std::max<size_t>(ni_total, 1), std::max<size_t>(parts, 1), nb)) return -3;
-    unsigned *d_status = reinterpret_cast<unsigned *>(d_out_);
-    cudaMemsetAsync(d_out_, 0, 16, stream_);
-    cudaEventRecord(ev_clear_, stream_);
-    // per call: i-records, item, outputs
-    size_t ioff = 0, poff = 0;
+    if (ensure(L, std::max<size_t>(ni_total, 1), std::max<size_t>(parts, 1), std::max<size_t>(jbytes, 256), nb))
+        return -3;
+    unsigned *d_status = reinterpret_cast<unsigned *>(L.d_out);
+    cudaMemsetAsync(L.d_out, 0, 16, L.stream);
+    cudaEventRecord(L.ev_clear, L.stream);
+    size_t ioff = 0, poff = 0, joff = 0;
     int task = 0;
     bool ident = true;
-    double *oacc = reinterpret_cast<double *>(d_out_ + 16);
+    double *oacc = reinterpret_cast<double *>(L.d_out + 16);
     double *ojerk = oacc + 3 * ni_total;
     double *opot = ojerk + 3 * ni_total;
     int *onn = reinterpret_cast<int *>(opot + ni_total);
@@ -394,18 +424,19 @@ int Server::run_batch(std::vector<std::shared_ptr<Request>> &batch) {
             cl = clusters_[r.cluster].get();
         }
         ForceParams p{};
+        const int nj_pad = (r.nj + T - 1) / T * T;
         {
             std::lock_guard<std::mutex> lk(cl->mu);
-            cl->eng->wait_event(ev_clear_);
+            cl->eng->wait_event(L.ev_clear);
             cl->eng->set_ti(r.ti);
             if (cl->eng->prepare_batch_item(r.nj, r.ni, reinterpret_cast<const double(*)[3]>(r.xi.data()), p,
-                                            cl->ready, d_status))
+                                            L.ready[k], d_status, L.d_jrec + joff))
                 return -2;
             ident &= cl->eng->identity_index();
         }
-        cudaStreamWaitEvent(stream_, cl->ready, 0);
+        cudaStreamWaitEvent(L.stream, L.ready[k], 0);
         for (int i = 0; i < r.ni; ++i) {
-            IRec &q = h_irec_[ioff + i];
+            IRec &q = L.h_irec[ioff + i];
             for (int c = 0; c < 3; ++c) {
                 q.x[c] = r.xi[3 * i + c];
                 q.v[c] = r.vi[3 * i + c];
@@ -414,10 +445,10 @@ int Server::run_batch(std::vector<std::shared_ptr<Request>> &batch) {
             q.index = r.index[i];
             q.pad = 0;
         }
-        p.irec = d_irec_ + ioff;
+        p.irec = L.d_irec + ioff;
         p.ni = r.ni;
         p.eps2 = r.eps2;
-        p.part = d_part_ + poff;
+        p.part = L.d_part + poff;
         p.out_acc = oacc + 3 * ioff;
         p.out_jerk = ojerk + 3 * ioff;
         p.out_pot = opot + ioff;
@@ -425,36 +456,39 @@ int Server::run_batch(std::vector<std::shared_ptr<Request>> &batch) {
         p.status = d_status;
         int nt = 0;
         batch_plan(kmode_, cfg_, p, nt);
-        h_items_[k] = p;
-        h_pre_[k] = task;
-        h_pre_[nb + 1 + k] = (int)ioff;
+        L.h_items[k] = p;
+        L.h_pre[k] = task;
+        L.h_pre[nb + 1 + k] = (int)ioff;
         task += nt;
         ioff += r.ni;
-        const int nj_pad = p.nj_pad;
         poff += (size_t)r.ni * batch_max_split(kmode_, nj_pad);
+        joff += (size_t)nj_pad * rec;
     }
-    h_pre_[nb] = task;
-    h_pre_[2 * nb + 1] = (int)ioff;
-    cudaEventRecord(ev_t0_, stream_);
-    cudaMemcpyAsync(d_irec_, h_irec_, sizeof(IRec) * ni_total, cudaMemcpyHostToDevice, stream_);
-    cudaMemcpyAsync(d_items_, h_items_, sizeof(ForceParams) * nb, cudaMemcpyHostToDevice, stream_);
-    cudaMemcpyAsync(d_pre_, h_pre_, sizeof(int) * 2 * (nb + 1), cudaMemcpyHostToDevice, stream_);
-    cudaMemsetAsync(d_counter_, 0, sizeof(int), stream_);
+    L.h_pre[nb] = task;
+    L.h_pre[2 * nb + 1] = (int)ioff;
+    cudaEventRecord(L.ev_t0, L.stream);
+    cudaMemcpyAsync(L.d_irec, L.h_irec, sizeof(IRec) * ni_total, cudaMemcpyHostToDevice, L.stream);
+    cudaMemcpyAsync(L.d_items, L.h_items, sizeof(ForceParams) * nb, cudaMemcpyHostToDevice, L.stream);
+    cudaMemcpyAsync(L.d_pre, L.h_pre, sizeof(int) * 2 * (nb + 1), cudaMemcpyHostToDevice, L.stream);
+    if (L.persistent) cudaMemsetAsync(L.d_counter, 0, sizeof(int), L.stream);
     BatchArgs a;
-    a.items = d_items_;
-    a.task0 = d_pre_;
-    a.ipre = d_pre_ + nb + 1;
+    a.items = L.d_items;
+    a.task0 = L.d_pre;
+    a.ipre = L.d_pre + nb + 1;
     a.n_items = nb;
     a.H = cfg_.H;
-    a.counter = d_counter_;
-    cudaError_t e = launch_force_batch(stream_, kmode_, cfg_, a, ctas_, (int)ni_total, false, ident);
+    a.counter = L.d_counter;
+    a.one_task_per_cta = L.persistent ? 0 : 1;
+    cudaError_t e = cudaSuccess;
+    if (task > 0)
+        e = launch_force_batch(L.stream, kmode_, cfg_, a, L.persistent ? ctas_ : task, (int)ni_total, false, ident);
     if (e != cudaSuccess) return -3;
-    cudaMemcpyAsync(h_out_, d_out_, 16 + 60 * ni_total, cudaMemcpyDeviceToHost, stream_);
-    cudaEventRecord(ev_t1_, stream_);
-    if (cudaStreamSynchronize(stream_) != cudaSuccess) return -3;
+    cudaMemcpyAsync(L.h_out, L.d_out, 16 + 60 * ni_total, cudaMemcpyDeviceToHost, L.stream);
+    cudaEventRecord(L.ev_t1, L.stream);
+    if (cudaStreamSynchronize(L.stream) != cudaSuccess) return -3;
     float ms = 0;
-    cudaEventElapsedTime(&ms, ev_t0_, ev_t1_);
-    const unsigned status = *reinterpret_cast<unsigned *>(h_out_);
+    cudaEventElapsedTime(&ms, L.ev_t0, L.ev_t1);
+    const unsigned status = *reinterpret_cast<unsigned *>(L.h_out);
     long long inter = 0;
     if (status & ST_RANGE) {
         // rare: redo each call alone with a widened fixed-point range
@@ -481,7 +515,7 @@ int Server::run_batch(std::vector<std::shared_ptr<Request>> &batch) {
             inter += (long long)r.ni * r.nj;
         }
     } else {
-        const unsigned char *base = h_out_ + 16;
+        const unsigned char *base = L.h_out + 16;
         const double *hacc = reinterpret_cast<const double *>(base);
         const double *hjerk = hacc + 3 * ni_total;
         const double *hpot = hjerk + 3 * ni_total;
