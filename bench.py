@@ -218,14 +218,15 @@ def served_section(seed):
                                    "interactions_per_s": inter2 / wall2}}
 
 
-def cpu_baseline(n, seed, cores):
-    """Starlab's FP64 force loop on a bounded sample of i (rank 0, N=1)."""
+def cpu_baseline(n, seed, cores, per_core=640):
+    """Starlab's FP64 force loop on a bounded sample of i (rank 0, N=1):
+    per_core i-particles per host thread against all N j."""
     m, x, v = make_cluster(n, seed)
     z = np.zeros((n, 3))
     try:
         from oracle.oracle import RefForce
         ref = RefForce()
-        ni = int(min(n, 640 * cores))
+        ni = int(min(n, per_core * cores))
         ilist = np.linspace(0, n - 1, ni).astype(np.int32)
         out = ref.force(m, x, v, z, z, 0.0, 0.0, float(np.sqrt(EPS2)), ilist=ilist, nthreads=cores)
         secs = out["seconds"]
@@ -253,7 +254,7 @@ def run_reference(args, dist):
     vals = []
     last = None
     for k in range(args.warmup + args.steps):
-        r = cpu_baseline(n, 11, cores)
+        r = cpu_baseline(n, 11, cores, per_core=96)
         if k >= args.warmup:
             vals.append(r["value"])
         last = r

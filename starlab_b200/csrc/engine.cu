@@ -16,6 +16,7 @@
 // hdyn_grape6.C drives (send_j_node_to_grape :273, force_by_grape :474-910).
 #include "engine.h"
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -66,6 +67,7 @@ Engine::Engine(int cluster_id) : cluster_id_(cluster_id) {
     const char *ml = getenv("G6B200_MIXED_LAYOUT");
     if (ml && !strcmp(ml, "scalar")) mixed_layout_ = kKernMixedDS;
     fault_lasthalf_at_ = env_ll("G6B200_FAULT_LASTHALF", -1);
+    event_timing_ = getenv("G6B200_EVENT_TIMING") != nullptr;
     fault_pot_at_ = env_ll("G6B200_FAULT_POT", -1);
 }
 
@@ -107,13 +109,20 @@ int Engine::open(int device, int nmax_hint) {
 
 void Engine::close() {
     if (!open_) return;
+    if (getenv("G6B200_TRACE")) {
+        fprintf(stderr,
+                "g6b200[%d] trace: calls %lld interactions %lld launches %lld predictions %lld nb_calls %lld "
+                "range_retries %lld grows %lld wait_ms %.1f host_ms %.1f mode %d\n",
+                cluster_id_, stats_.calls, stats_.interactions, stats_.launches, stats_.predictions, stats_.nb_calls,
+                stats_.range_retries, stats_.grows, stats_.wait_ms, stats_.host_ms, mode_);
+    }
     cudaSetDevice(device_);
     cudaStreamSynchronize(stream_);
     auto dfree = [](void *p) { if (p) cudaFree(p); };
     auto hfree = [](void *p) { if (p) cudaFreeHost(p); };
     dfree(d_jraw_); dfree(d_jindex_); dfree(d_jrec_);
     dfree(d_stage_vals_); dfree(d_stage_addr_); dfree(d_stage_index_);
-    dfree(d_irec_); dfree(d_out_); dfree(d_part_);
+    dfree(d_irec_); dfree(d_out_); dfree(d_part_); dfree(d_tile_cnt_);
     dfree(d_nb_count_); dfree(d_nb_list_); dfree(d_nb_sorted_); dfree(d_nb_off_);
     hfree(h_stage_vals_); hfree(h_stage_addr_); hfree(h_stage_index_);
     hfree(h_irec_); hfree(h_out_); hfree(h_nb_off_); hfree(h_nb_count_);
@@ -122,7 +131,7 @@ void Engine::close() {
     cudaStreamDestroy(stream_);
     d_jraw_ = nullptr; d_jindex_ = nullptr; d_jrec_ = nullptr;
     d_stage_vals_ = nullptr; d_stage_addr_ = nullptr; d_stage_index_ = nullptr;
-    d_irec_ = nullptr; d_out_ = nullptr; d_part_ = nullptr;
+    d_irec_ = nullptr; d_out_ = nullptr; d_part_ = nullptr; d_tile_cnt_ = nullptr;
     d_nb_count_ = nullptr; d_nb_list_ = nullptr; d_nb_sorted_ = nullptr; d_nb_off_ = nullptr;
     h_stage_vals_ = nullptr; h_stage_addr_ = nullptr; h_stage_index_ = nullptr;
     h_irec_ = nullptr; h_out_ = nullptr; h_nb_off_ = nullptr; h_nb_count_ = nullptr;
@@ -139,6 +148,10 @@ int Engine::reset() {
     cudaSetDevice(device_);
     cudaStreamSynchronize(stream_);
     cudaGetLastError();  // clear a sticky non-fatal error, if any
+    if (d_tile_cnt_) {
+        cudaMemsetAsync(d_tile_cnt_, 0, sizeof(int) * call_cap_, stream_);
+        cudaStreamSynchronize(stream_);
+    }
     for (int k = 0; k < n_staged_; ++k) slot_of_[h_stage_addr_[k]] = -1;
     n_staged_ = 0;
     pending_ = false;
@@ -276,6 +289,7 @@ FixedScale Engine::scale() const {
 }
 
 int Engine::ensure_call_buffers(int ni, bool nb, size_t part_bytes) {
+    if (ni > call_cap_ || part_bytes > part_cap_ || (nb && nb_alloc_ < std::max(call_cap_, ni))) stats_.grows++;
     if (ni > call_cap_) {
         int ncap = std::max(ni, npipes_);
         if (h_irec_) cudaFreeHost(h_irec_);
@@ -289,6 +303,10 @@ int Engine::ensure_call_buffers(int ni, bool nb, size_t part_bytes) {
         G6_CHECK(cudaMalloc(&d_irec_, sizeof(IRec) * ncap), "i-records");
         G6_CHECK(cudaMallocHost(&h_out_, L.total), "pinned out");
         G6_CHECK(cudaMalloc(&d_out_, L.total), "out");
+        if (d_tile_cnt_) cudaFree(d_tile_cnt_);
+        d_tile_cnt_ = nullptr;
+        G6_CHECK(cudaMalloc(&d_tile_cnt_, sizeof(int) * ncap), "tile counters");
+        G6_CHECK(cudaMemsetAsync(d_tile_cnt_, 0, sizeof(int) * ncap, stream_), "memset");
         call_cap_ = ncap;
     }
     if (part_bytes > part_cap_) {
@@ -319,6 +337,14 @@ int Engine::ensure_call_buffers(int ni, bool nb, size_t part_bytes) {
 
 int Engine::firsthalf(int nj, int ni, const int *index, const double (*xi)[3], const double (*vi)[3],
                       double eps2, const double *h2) {
+    const auto h0 = std::chrono::steady_clock::now();
+    struct HostTimer {
+        EngineStats &st;
+        std::chrono::steady_clock::time_point t0;
+        ~HostTimer() {
+            st.host_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+        }
+    } host_timer{stats_, h0};
     call_error_ = false;
     if (!open_ && open(env_int("G6B200_DEVICE", 0), 0)) {
         call_error_ = true;
@@ -396,16 +422,18 @@ int Engine::launch_call() {
     }
     const FixedScale fs = scale();
     OutLayout L(ni);
-    G6_CHECK(cudaEventRecord(ev_begin_, stream_), "event");
+    timed_ = event_timing_ || call_sweep_;
+    if (timed_) G6_CHECK(cudaEventRecord(ev_begin_, stream_), "event");
     G6_CHECK(cudaMemsetAsync(d_out_, 0, 16, stream_), "memset");
     unsigned *status = reinterpret_cast<unsigned *>(d_out_ + L.status);
     pred_timed_ = false;
     if (!pred_valid_ || pred_ti_ != ti_ || pred_nj_ != nj || pred_mode_ != km || pred_E_ != E_) {
-        G6_CHECK(cudaEventRecord(ev_pred0_, stream_), "event");
+        if (timed_) G6_CHECK(cudaEventRecord(ev_pred0_, stream_), "event");
         launch_predict(stream_, km, d_jraw_, d_jindex_, cap_, nj, nj_pad, ti_, fs, d_jrec_, status);
         G6_CHECK(cudaGetLastError(), "predict launch");
         stats_.launches++;
-        G6_CHECK(cudaEventRecord(ev_pred1_, stream_), "event");
+        if (timed_) G6_CHECK(cudaEventRecord(ev_pred1_, stream_), "event");
+        stats_.predictions++;
         pred_timed_ = true;
         pred_valid_ = true;
         pred_ti_ = ti_;
@@ -444,12 +472,14 @@ int Engine::launch_call() {
         p.nb_cap = nb_cap_;
         p.include_self = npipes_ > 48;
         p.status = status;
+        p.tile_counter = d_tile_cnt_;
         if (call_nb_) G6_CHECK(cudaMemsetAsync(d_nb_count_, 0, sizeof(int) * ni, stream_), "memset");
-        G6_CHECK(cudaEventRecord(ev_force0_, stream_), "event");
+        if (timed_) G6_CHECK(cudaEventRecord(ev_force0_, stream_), "event");
         G6_CHECK(launch_force(stream_, km, cfg, p, n_nonident_ == 0, call_nb_), "force launch");
-        G6_CHECK(cudaEventRecord(ev_force1_, stream_), "event");
-        stats_.launches += 1 + (partial_bytes(cfg, ni) > 0 ? 1 : 0);
+        if (timed_) G6_CHECK(cudaEventRecord(ev_force1_, stream_), "event");
+        stats_.launches += 1;
         if (call_nb_) {
+            stats_.nb_calls++;
             G6_CHECK(launch_nb_compact(stream_, ni, d_nb_count_, d_nb_list_, nb_cap_, d_nb_off_, d_nb_sorted_),
                      "nb compact");
             stats_.launches += 2;
@@ -458,7 +488,7 @@ int Engine::launch_call() {
             G6_CHECK(cudaMemcpyAsync(h_nb_count_, d_nb_count_, sizeof(int) * ni, cudaMemcpyDeviceToHost, stream_),
                      "nb copy");
         }
-    } else {
+    } else if (timed_) {
         G6_CHECK(cudaEventRecord(ev_force0_, stream_), "event");
         G6_CHECK(cudaEventRecord(ev_force1_, stream_), "event");
     }
@@ -498,7 +528,9 @@ int Engine::lasthalf(int ni, double (*acc)[3], double (*jerk)[3], double *pot, i
 int Engine::wait_call() {
     G6_CHECK(cudaSetDevice(device_), "cudaSetDevice");
     for (int attempt = 0;; ++attempt) {
+        const auto w0 = std::chrono::steady_clock::now();
         cudaError_t e = cudaEventSynchronize(ev_done_);
+        stats_.wait_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - w0).count();
         if (e != cudaSuccess) {
             fail("device execution", e);
             return 2;
@@ -506,6 +538,7 @@ int Engine::wait_call() {
         unsigned status = *reinterpret_cast<unsigned *>(h_out_);
         if ((status & ST_RANGE) && attempt < 8) {
             // Fixed-point range exceeded: widen by 4x and recompute.
+            stats_.range_retries++;
             E_ += 2;
             pred_valid_ = false;
             if (launch_call()) return 2;
@@ -522,6 +555,10 @@ int Engine::wait_call() {
         break;
     }
     float ms = 0;
+    if (!timed_) {
+        stats_.last_force_ms = stats_.last_predict_ms = stats_.last_call_ms = 0;
+        return 0;
+    }
     if (cudaEventElapsedTime(&ms, ev_force0_, ev_force1_) == cudaSuccess) stats_.last_force_ms = ms;
     if (pred_timed_ && cudaEventElapsedTime(&ms, ev_pred0_, ev_pred1_) == cudaSuccess)
         stats_.last_predict_ms = ms;

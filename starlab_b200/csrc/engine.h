@@ -17,6 +17,9 @@ struct EngineStats {
     double last_predict_ms = 0;
     double last_call_ms = 0;
     long long launches = 0;  // kernels launched by this instance
+    // diagnostics (G6B200_TRACE=1 prints them when the instance closes)
+    long long range_retries = 0, nb_calls = 0, predictions = 0, grows = 0;
+    double wait_ms = 0, host_ms = 0;
 };
 
 class Engine {
@@ -135,6 +138,9 @@ class Engine {
     unsigned char *h_out_ = nullptr, *d_out_ = nullptr;
     size_t part_cap_ = 0;
     Partial *d_part_ = nullptr;
+    int *d_tile_cnt_ = nullptr;  // [call_cap_] i-tile arrival counters, kept at zero
+    bool event_timing_ = false;  // per-call timing events (G6B200_EVENT_TIMING; sweeps always)
+    bool timed_ = false;         // this call records timing events
 
     // neighbour lists
     int nb_alloc_ = 0;

@@ -488,6 +488,20 @@ __device__ __forceinline__ void warp_reduce(Partial &q) {
     }
 }
 
+// Partial written by another CTA of the same launch: read around L1.
+__device__ __forceinline__ Partial load_partial_cg(const Partial *src) {
+    Partial a;
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+        a.acc[c] = __ldcg(&src->acc[c]);
+        a.jerk[c] = __ldcg(&src->jerk[c]);
+    }
+    a.pot = __ldcg(&src->pot);
+    a.nn_r2 = __ldcg(&src->nn_r2);
+    a.nn_j = __ldcg(&src->nn_j);
+    return a;
+}
+
 __device__ __forceinline__ void write_final(const ForceParams &p, int i, const Partial &q) {
 #pragma unroll
     for (int c = 0; c < 3; c++) {
@@ -617,6 +631,26 @@ __device__ __forceinline__ void process_task(const ForceParams &p, int itile_idx
                 write_final(p, i, q[r]);
             else
                 p.part[(size_t)split * p.ni + i] = q[r];
+        }
+    }
+    if (p.nsplit > 1 && p.tile_counter) {
+        // Last CTA of this i-tile folds the splits (threadfence reduction).
+        __shared__ int s_last;
+        __threadfence();
+        __syncthreads();
+        if (threadIdx.x == 0) s_last = atomicAdd(&p.tile_counter[itile_idx], 1) == p.nsplit - 1;
+        __syncthreads();
+        if (s_last) {
+            __threadfence();
+            const int ib = itile_idx * itile;
+            for (int k = threadIdx.x; k < itile; k += blockDim.x) {
+                const int i = ib + k;
+                if (i >= p.ni) continue;
+                Partial a = load_partial_cg(p.part + i);
+                for (int sp = 1; sp < p.nsplit; ++sp) add_partial(a, load_partial_cg(p.part + (size_t)sp * p.ni + i));
+                write_final(p, i, a);
+            }
+            if (threadIdx.x == 0) p.tile_counter[itile_idx] = 0;
         }
     }
 }
@@ -856,7 +890,7 @@ cudaError_t launch_force(cudaStream_t s, int kmode, const ForceConfig &cfg, Forc
     fn<<<grid, block, sm, s>>>(p);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
-    if (p.nsplit > 1) {
+    if (p.nsplit > 1 && !p.tile_counter) {
         reduce_partials_kernel<<<(p.ni + 255) / 256, 256, 0, s>>>(p);
         e = cudaGetLastError();
     }

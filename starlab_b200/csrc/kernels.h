@@ -56,6 +56,11 @@ struct ForceParams {
     int nb_cap;
     int include_self;
     unsigned *status;
+    // Per-i-tile arrival counters (zero between calls).  When set and
+    // nsplit > 1, the last CTA of an i-tile adds the split partials in split
+    // order and writes the results, so no separate reduction launch is needed;
+    // it leaves its counter at zero again.
+    int *tile_counter;
 };
 
 // A batch of calls for the persistent multi-item kernel (device pointers).

@@ -10,6 +10,7 @@ under a profiler on a bounded case.
 """
 import argparse
 import json
+import os
 
 import numpy as np
 
@@ -26,6 +27,7 @@ def main():
     ap.add_argument("--h2", type=float, default=0.0)
     ap.add_argument("--config", default="", help="il,r,warps,h,nsplit")
     a = ap.parse_args()
+    os.environ.setdefault("G6B200_EVENT_TIMING", "1")  # per-call device times in the stats
     m, x, v = ics.plummer(a.n, 11, masses=ics.salpeter_masses(a.n, 12))
     z = np.zeros((a.n, 3))
     eng = G6Engine(cluster_id=0, precision=a.mode, npipes=max(a.ni, 1))
