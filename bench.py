@@ -218,9 +218,16 @@ def served_section(seed):
                                    "interactions_per_s": inter2 / wall2}}
 
 
-def cpu_baseline(n, seed, cores, per_core=640):
+def _rel(a, b):
+    return np.linalg.norm(a - b, axis=1) / np.linalg.norm(b, axis=1) if a.ndim == 2 else np.abs(a - b) / np.abs(b)
+
+
+def cpu_baseline(n, seed, cores, per_core=640, gpu=None):
     """Starlab's FP64 force loop on a bounded sample of i (rank 0, N=1):
-    per_core i-particles per host thread against all N j."""
+    per_core i-particles per host thread against all N j.  When `gpu` holds
+    the engine's (acc, jerk, pot, nn) for every particle of the same state
+    (t = 0, no prediction), the reference's results for the sample also score
+    them: per-particle relative error of acc, jerk and pot, nn mismatches."""
     m, x, v = make_cluster(n, seed)
     z = np.zeros((n, 3))
     try:
@@ -230,9 +237,19 @@ def cpu_baseline(n, seed, cores, per_core=640):
         ilist = np.linspace(0, n - 1, ni).astype(np.int32)
         out = ref.force(m, x, v, z, z, 0.0, 0.0, float(np.sqrt(EPS2)), ilist=ilist, nthreads=cores)
         secs = out["seconds"]
-        return {"value": ni * (n - 1) / secs, "unit": "interactions/s", "cores": cores, "kind": "reference",
-                "sample": "%d i (evenly spaced) x %d j, hdyn::flat_calculate_acc_and_jerk on %d threads; "
-                          "force loop %.2f s" % (ni, n, cores, secs)}
+        res = {"value": ni * (n - 1) / secs, "unit": "interactions/s", "cores": cores, "kind": "reference",
+               "sample": "%d i (evenly spaced) x %d j, hdyn::flat_calculate_acc_and_jerk on %d threads; "
+                         "force loop %.2f s" % (ni, n, cores, secs)}
+        if gpu is not None:
+            acc, jerk, pot, nn = (g[ilist] for g in gpu)
+            acc_err, jerk_err, pot_err = _rel(acc, out["acc"]), _rel(jerk, out["jerk"]), _rel(pot, out["pot"])
+            res["accuracy_vs_reference"] = {
+                "sample_i": int(ni), "precision": "mixed",
+                "acc": {"median": float(np.median(acc_err)), "max": float(acc_err.max())},
+                "jerk": {"median": float(np.median(jerk_err)), "max": float(jerk_err.max())},
+                "pot": {"median": float(np.median(pot_err)), "max": float(pot_err.max())},
+                "nn_mismatch": int(np.sum(nn != out["nn"]))}
+        return res
     except ImportError:
         from oracle.oracle import G6Oracle
         o = G6Oracle()
@@ -420,7 +437,7 @@ def main():
         if dist.world == 1 and not args.no_served:
             line["served_stream"] = served_section(5)
         if dist.world == 1 and not args.no_cpu_baseline:
-            line["cpu_baseline"] = cpu_baseline(n, seed, os.cpu_count() or 1)
+            line["cpu_baseline"] = cpu_baseline(n, seed, os.cpu_count() or 1, gpu=(acc, jerk, pot, nn))
         print(json.dumps(line), flush=True)
     for e in (eng, eng2, eng3):
         e.close()
