@@ -21,7 +21,15 @@ with g++ directly (no autotools: they are absent here), into ``oracle/_ref/``:
 * ``libref_force.so``  ``oracle/ref_force.C``: a C entry point over the
                        reference's ``predict_loworder`` and
                        ``hdyn::flat_calculate_acc_and_jerk``
-                       (``src/node/dyn/hdyn/evolve/hdyn_ev.C:2047``).
+                       (``src/node/dyn/hdyn/evolve/hdyn_ev.C:2047``);
+* ``libharp3sim.so``   the reference's IEEE GRAPE-4 simulator
+                       (``src/harpsims/harp3fastsim.c``), compiled as it is
+                       (K&R C: ``-std=gnu89``), the executable definition of
+                       the GRAPE-4 ABI;
+* ``kira_g4``/``hsys_stats_g4``  the mains linked against ``libh3b200.so``,
+                       with ``hdyn_grape4.C`` recompiled under
+                       ``USE_HALF_CHIP`` as configure defines it when it finds
+                       a GRAPE-4 library (``configure.ac:216-222``).
 
 Nothing here is shipped; the outputs are git-ignored.  Usage:
 ``python oracle/build_ref.py [--jobs N] [--ref PATH]``.
@@ -150,6 +158,11 @@ def main():
         tool_objs[name] = obj
     harness_obj = os.path.join(OUT, "obj", "ref_force.o")
     add(os.path.join(HERE, "ref_force.C"), harness_obj)
+    g4_obj = os.path.join(OUT, "obj", "hdyn_grape4_half_chip.o")
+    add(os.path.join(src, "node/dyn/hdyn/evolve/hdyn_grape4.C"), g4_obj, extra=["-DUSE_HALF_CHIP=1"])
+    sim_src = os.path.join(src, "harpsims", "harp3fastsim.c")
+    sim_obj = os.path.join(OUT, "obj", "harp3fastsim.o")
+    add(sim_src, sim_obj, extra=["-std=gnu89"], c=True)
 
     todo = [j for j in jobs if not up_to_date(j[0], j[2])]
     if not args.quiet:
@@ -178,6 +191,10 @@ def main():
         run(["g++", "-shared", "-o", so, harness_obj, "-Wl,--whole-archive", lib,
              "-Wl,--no-whole-archive", stubs] + link_tail)
 
+    sim_so = os.path.join(OUT, "libharp3sim.so")
+    if not up_to_date(sim_so, [sim_obj]):
+        run(["gcc", "-shared", "-o", sim_so, sim_obj, "-lm"])
+
     # kira and hsys_stats driving the GPU engine through the unchanged g6 ABI.
     g6lib_dir = os.path.join(REPO, "starlab_b200", "lib")
     g6lib = os.path.join(g6lib_dir, "libg6b200.so")
@@ -187,6 +204,15 @@ def main():
             exe = os.path.join(OUT, name + "_g6")
             if not up_to_date(exe, [tool_objs[name], lib, stubs, g6lib]):
                 run(["g++", "-o", exe, tool_objs[name], lib, "-L" + g6lib_dir, "-lg6b200",
+                     rpath, stubs] + link_tail)
+    # The same mains on the GRAPE-4 ABI (kira's config == 1 branch).
+    h3lib = os.path.join(g6lib_dir, "libh3b200.so")
+    if os.path.exists(h3lib):
+        rpath = "-Wl,-rpath,$ORIGIN/../../starlab_b200/lib"
+        for name in ("kira", "hsys_stats", "hscale"):
+            exe = os.path.join(OUT, name + "_g4")
+            if not up_to_date(exe, [tool_objs[name], g4_obj, lib, stubs, h3lib]):
+                run(["g++", "-o", exe, tool_objs[name], g4_obj, lib, "-L" + g6lib_dir, "-lh3b200",
                      rpath, stubs] + link_tail)
     if not args.quiet:
         print("oracle/_ref: done")

@@ -5,6 +5,10 @@
 * ``RefForce``  -- oracle/_ref/libref_force.so, Starlab's own FP64 path
   (predict_loworder + hdyn::flat_calculate_acc_and_jerk) built from the
   reference sources by oracle/build_ref.py.
+* ``G4Oracle``  -- oracle/_build/libg4oracle.so, the FP64 C restatement of
+  the GRAPE-4 pipeline (oracle/g4_oracle.c).
+* ``Harp3Sim``  -- oracle/_ref/libharp3sim.so, the reference's own IEEE
+  GRAPE-4 simulator (src/harpsims/harp3fastsim.c) driven through its ABI.
 """
 import ctypes
 import os
@@ -14,6 +18,8 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_LIB = os.path.join(HERE, "_build", "libg6oracle.so")
 REF_LIB = os.path.join(HERE, "_ref", "libref_force.so")
+G4_ORACLE_LIB = os.path.join(HERE, "_build", "libg4oracle.so")
+HARP3_LIB = os.path.join(HERE, "_ref", "libharp3sim.so")
 
 _P = ctypes.c_void_p
 
@@ -105,3 +111,90 @@ class RefForce:
         if want_pred:
             out["pred_pos"], out["pred_vel"] = pp, pv
         return out
+
+
+class G4Oracle:
+    """GRAPE-4 pipeline restated in C (predictor and pair loop of
+    harp3fastsim.c, plus the potential the simulator leaves at 0)."""
+
+    def __init__(self, path=G4_ORACLE_LIB):
+        if not os.path.exists(path):
+            raise ImportError("oracle library missing: %s" % path)
+        self.lib = ctypes.CDLL(path)
+        I, D = ctypes.c_int, ctypes.c_double
+        self.lib.g4o_predict.argtypes = [I, D, _P, _P, _P, _P, _P, _P, _P]
+        self.lib.g4o_force.argtypes = [I, _P, _P, _P, I, _P, _P, _P, _P, _P, _P, _P, _P, _P, I]
+
+    def predict(self, ti, tj, x, v, aj, jj):
+        n = x.shape[0]
+        tj = _c(np.broadcast_to(np.asarray(tj, np.float64), (n,)))
+        xp, vp = np.empty((n, 3)), np.empty((n, 3))
+        self.lib.g4o_predict(n, float(ti), _p(tj), _p(_c(x)), _p(_c(v)), _p(_c(aj)), _p(_c(jj)), _p(xp), _p(vp))
+        return xp, vp
+
+    def force(self, xj, vj, mj, xi, vi, eps2, h2, nbcap=None):
+        """acc, jerk, pot and the neighbour lists (ascending) per i-slot."""
+        nj, ni = xj.shape[0], xi.shape[0]
+        eps2 = _c(np.broadcast_to(np.asarray(eps2, np.float64), (ni,)))
+        h2 = _c(np.broadcast_to(np.asarray(h2, np.float64), (ni,)))
+        acc, jerk, pot = np.empty((ni, 3)), np.empty((ni, 3)), np.empty(ni)
+        cnt = np.empty(ni, dtype=np.int32)
+        cap = nj if nbcap is None else nbcap
+        lists = np.empty((ni, max(cap, 1)), dtype=np.int32)
+        self.lib.g4o_force(nj, _p(_c(xj)), _p(_c(vj)), _p(_c(mj)), ni, _p(_c(xi)), _p(_c(vi)), _p(eps2), _p(h2),
+                           _p(acc), _p(jerk), _p(pot), _p(cnt), _p(lists), cap)
+        nb = [lists[i, :min(cnt[i], cap)].copy() for i in range(ni)]
+        return acc, jerk, pot, cnt, nb
+
+
+class Harp3Sim:
+    """The reference's GRAPE-4 simulator through its own ABI.
+
+    Its static limits (harp3fastsim.c:23-26, 31): 1000 j-particles, 3 i per
+    call, 26 j per DMA buffer, 1024 neighbours per i (unchecked: keep lists
+    shorter).  It returns pot = 0 (:281).
+    """
+    NMAX, IPMAX, JPMAX, NNBMAX = 1000, 3, 26, 1024
+
+    def __init__(self, path=HARP3_LIB):
+        if not os.path.exists(path):
+            raise ImportError("reference GRAPE-4 simulator not built: %s (python oracle/build_ref.py)" % path)
+        self.lib = ctypes.CDLL(path)
+        self.lib.h3nblist_.restype = ctypes.c_int
+
+    def _i(self, v):
+        return ctypes.byref(ctypes.c_int(int(v)))
+
+    def load(self, x, v, aj, jj, m, t):
+        n = x.shape[0]
+        assert n <= self.NMAX
+        x, v, aj, jj = _c(x), _c(v), _c(aj), _c(jj)
+        m = _c(m)
+        t = _c(np.broadcast_to(np.asarray(t, np.float64), (n,)))
+        for b0 in range(0, n, self.JPMAX):
+            idx = _c(np.arange(b0 + 1, min(b0 + self.JPMAX, n) + 1), np.int32)
+            self.lib.h3mjpdma_indirect_(self._i(idx.size), _p(idx), _p(x), _p(v), _p(aj), _p(jj), _p(m), _p(t),
+                                        self._i(1), self._i(0))
+            self.lib.h3mjpdma_start_(self._i(0))
+
+    def force(self, ti, nj, xi, vi, eps2, h2):
+        """acc, jerk and neighbour lists for every i (3 per call)."""
+        ni = xi.shape[0]
+        eps2 = _c(np.broadcast_to(np.asarray(eps2, np.float64), (ni,)))
+        h2 = _c(np.broadcast_to(np.asarray(h2, np.float64), (ni,)))
+        xi, vi = _c(xi), _c(vi)
+        self.lib.h3setti_(ctypes.byref(ctypes.c_double(float(ti))))
+        acc, jerk = np.empty((ni, 3)), np.empty((ni, 3))
+        lists = []
+        buf = np.empty(self.NNBMAX, dtype=np.int32)
+        for i0 in range(0, ni, self.IPMAX):
+            k = min(self.IPMAX, ni - i0)
+            a, jk, p = np.empty((k, 3)), np.empty((k, 3)), np.empty(k)
+            self.lib.h3calc_firsthalf_(self._i(nj), self._i(k), _p(_c(xi[i0:i0 + k])), _p(_c(vi[i0:i0 + k])),
+                                       _p(_c(eps2[i0:i0 + k])), _p(_c(h2[i0:i0 + k])))
+            self.lib.h3calc_lasthalf_(self._i(k), _p(a), _p(jk), _p(p))
+            acc[i0:i0 + k], jerk[i0:i0 + k] = a, jk
+            for c in range(k):
+                got = self.lib.h3nblist_(self._i(0), self._i(c), _p(buf))
+                lists.append(buf[:got].copy())
+        return acc, jerk, lists

@@ -1,9 +1,13 @@
 """Build the engine library and the oracle's C restatement in-tree.
 
-* ``starlab_b200/lib/libg6b200.so`` -- every ``csrc/*.cu`` compiled by nvcc
-  for sm_100a only (``-gencode arch=compute_100a,code=sm_100a``), linked as
-  one shared library exporting the C ABI of ``include/g6b200.h``.
-* ``oracle/_build/libg6oracle.so`` -- ``oracle/g6_oracle.c`` (test
+* ``starlab_b200/lib/libg6b200.so`` -- every ``csrc/*.cu`` but ``grape4.cu``
+  compiled by nvcc for sm_100a only (``-gencode arch=compute_100a,code=sm_100a``),
+  linked as one shared library exporting the C ABI of ``include/g6b200.h``.
+* ``starlab_b200/lib/libh3b200.so`` -- the GRAPE-4 ABI of ``include/h3b200.h``:
+  ``grape4.cu`` with the engine objects it drives (a library of its own, since
+  kira takes its GRAPE-4 branch whenever ``h3npipe_()`` answers).
+* ``oracle/_build/libg6oracle.so`` / ``libg4oracle.so`` -- the oracle's C
+  restatements ``oracle/g6_oracle.c`` and ``oracle/g4_oracle.c`` (test
   infrastructure) with gcc, FP contraction off.
 
 Usage: ``python -m starlab_b200.build [--verbose] [--ptxas-v]``.
@@ -20,8 +24,13 @@ CSRC = os.path.join(PKG, "csrc")
 LIBDIR = os.path.join(PKG, "lib")
 OBJDIR = os.path.join(PKG, "_build")
 LIB = os.path.join(LIBDIR, "libg6b200.so")
+LIB_H3 = os.path.join(LIBDIR, "libh3b200.so")
+H3_ONLY = {"grape4.o"}
+H3_OBJS = {"engine.o", "force.o", "predict.o", "nblist.o", "grape4.o"}
 ORACLE_SRC = os.path.join(REPO, "oracle", "g6_oracle.c")
 ORACLE_LIB = os.path.join(REPO, "oracle", "_build", "libg6oracle.so")
+ORACLE_G4_SRC = os.path.join(REPO, "oracle", "g4_oracle.c")
+ORACLE_G4_LIB = os.path.join(REPO, "oracle", "_build", "libg4oracle.so")
 
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -53,6 +62,7 @@ def build_engine(verbose=False, ptxas_v=False, force=False):
     srcs = sorted(f for f in os.listdir(CSRC) if f.endswith(".cu"))
     headers = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".h", ".cuh"))]
     headers.append(os.path.join(REPO, "include", "g6b200.h"))
+    headers.append(os.path.join(REPO, "include", "h3b200.h"))
     objs, jobs = [], []
     for f in srcs:
         src = os.path.join(CSRC, f)
@@ -66,15 +76,20 @@ def build_engine(verbose=False, ptxas_v=False, force=False):
     if ptxas_v:
         for o in outs:
             print(o)
-    if force or jobs or not _newer(LIB, objs):
-        _run([NVCC] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcudart"], verbose)
+    g6_objs = [o for o in objs if os.path.basename(o) not in H3_ONLY]
+    h3_objs = [o for o in objs if os.path.basename(o) in H3_OBJS]
+    if force or jobs or not _newer(LIB, g6_objs):
+        _run([NVCC] + ARCH + ["-shared", "-o", LIB] + g6_objs + ["-lcudart"], verbose)
+    if force or jobs or not _newer(LIB_H3, h3_objs):
+        _run([NVCC] + ARCH + ["-shared", "-o", LIB_H3] + h3_objs + ["-lcudart"], verbose)
     return LIB
 
 
 def build_oracle(verbose=False):
     os.makedirs(os.path.dirname(ORACLE_LIB), exist_ok=True)
-    if not _newer(ORACLE_LIB, [ORACLE_SRC]):
-        _run(["gcc", "-O2", "-fPIC", "-shared", "-ffp-contract=off", "-o", ORACLE_LIB, ORACLE_SRC, "-lm"], verbose)
+    for src, lib in ((ORACLE_SRC, ORACLE_LIB), (ORACLE_G4_SRC, ORACLE_G4_LIB)):
+        if not _newer(lib, [src]):
+            _run(["gcc", "-O2", "-fPIC", "-shared", "-ffp-contract=off", "-o", lib, src, "-lm"], verbose)
     return ORACLE_LIB
 
 

@@ -147,4 +147,12 @@ __device__ __forceinline__ float rsqrt_approx(float x) {
     return y;
 }
 
+// GRAPE-4 softened squared distance, eps2 + dx^2 + dy^2 + dz^2 accumulated
+// in that order (src/harpsims/harp3fastsim.c:270-272), as one fixed chain of
+// fused multiply-adds so that the force kernel and the full neighbour-list
+// pass round it identically (their neighbour tests then agree exactly).
+__device__ __forceinline__ double g4_r2(double dx, double dy, double dz, double eps2) {
+    return __fma_rn(dz, dz, __fma_rn(dy, dy, __fma_rn(dx, dx, eps2)));
+}
+
 }  // namespace g6

@@ -126,6 +126,7 @@ void Engine::close() {
     dfree(d_nb_count_); dfree(d_nb_list_); dfree(d_nb_sorted_); dfree(d_nb_off_);
     hfree(h_stage_vals_); hfree(h_stage_addr_); hfree(h_stage_index_);
     hfree(h_irec_); hfree(h_out_); hfree(h_nb_off_); hfree(h_nb_count_);
+    hfree(h_ieps2_); dfree(d_ieps2_);
     cudaEvent_t evs[] = {ev_stage_, ev_begin_, ev_pred0_, ev_pred1_, ev_force0_, ev_force1_, ev_done_};
     for (cudaEvent_t e : evs) if (e) cudaEventDestroy(e);
     cudaStreamDestroy(stream_);
@@ -135,6 +136,7 @@ void Engine::close() {
     d_nb_count_ = nullptr; d_nb_list_ = nullptr; d_nb_sorted_ = nullptr; d_nb_off_ = nullptr;
     h_stage_vals_ = nullptr; h_stage_addr_ = nullptr; h_stage_index_ = nullptr;
     h_irec_ = nullptr; h_out_ = nullptr; h_nb_off_ = nullptr; h_nb_count_ = nullptr;
+    h_ieps2_ = nullptr; d_ieps2_ = nullptr;
     ev_stage_ = ev_begin_ = ev_pred0_ = ev_pred1_ = ev_force0_ = ev_force1_ = ev_done_ = nullptr;
     stream_ = nullptr;
     cap_ = 0; call_cap_ = 0; part_cap_ = 0; nb_alloc_ = 0;
@@ -296,11 +298,16 @@ int Engine::ensure_call_buffers(int ni, bool nb, size_t part_bytes) {
         if (d_irec_) cudaFree(d_irec_);
         if (h_out_) cudaFreeHost(h_out_);
         if (d_out_) cudaFree(d_out_);
+        if (h_ieps2_) cudaFreeHost(h_ieps2_);
+        if (d_ieps2_) cudaFree(d_ieps2_);
         h_irec_ = d_irec_ = nullptr;
         h_out_ = d_out_ = nullptr;
+        h_ieps2_ = d_ieps2_ = nullptr;
         OutLayout L(ncap);
         G6_CHECK(cudaMallocHost(&h_irec_, sizeof(IRec) * ncap), "pinned i");
         G6_CHECK(cudaMalloc(&d_irec_, sizeof(IRec) * ncap), "i-records");
+        G6_CHECK(cudaMallocHost(&h_ieps2_, sizeof(double) * ncap), "pinned i");
+        G6_CHECK(cudaMalloc(&d_ieps2_, sizeof(double) * ncap), "i-softening");
         G6_CHECK(cudaMallocHost(&h_out_, L.total), "pinned out");
         G6_CHECK(cudaMalloc(&d_out_, L.total), "out");
         if (d_tile_cnt_) cudaFree(d_tile_cnt_);
@@ -337,6 +344,21 @@ int Engine::ensure_call_buffers(int ni, bool nb, size_t part_bytes) {
 
 int Engine::firsthalf(int nj, int ni, const int *index, const double (*xi)[3], const double (*vi)[3],
                       double eps2, const double *h2) {
+    return firsthalf_impl(nj, ni, index, xi, vi, eps2, nullptr, h2);
+}
+
+int Engine::firsthalf_g4(int nj, int ni, const double (*xi)[3], const double (*vi)[3], const double *eps2,
+                         const double *h2) {
+    if (mode_ != kModeF64) {
+        call_error_ = true;
+        last_error = "g6b200: the GRAPE-4 pipeline runs in FP64 mode only";
+        return -1;
+    }
+    return firsthalf_impl(nj, ni, nullptr, xi, vi, 0.0, eps2, h2);
+}
+
+int Engine::firsthalf_impl(int nj, int ni, const int *index, const double (*xi)[3], const double (*vi)[3],
+                           double eps2, const double *ieps2, const double *h2) {
     const auto h0 = std::chrono::steady_clock::now();
     struct HostTimer {
         EngineStats &st;
@@ -384,14 +406,16 @@ int Engine::firsthalf(int nj, int ni, const int *index, const double (*xi)[3], c
             if (ax > xm) xm = ax;
         }
         r.h2 = h2 ? h2[i] : default_h2_;
-        r.index = index[i];
+        r.index = index ? index[i] : -1;
         r.pad = 0;
+        if (ieps2) h_ieps2_[i] = ieps2[i];
     }
     xmax_ = xm;
     call_ni_ = ni;
     call_nj_ = nj;
     call_eps2_ = eps2;
     call_nb_ = nb;
+    call_g4_ = ieps2 != nullptr;
     call_sweep_ = false;
     call_copy_ = true;
     call_i0_ = 0;
@@ -450,6 +474,11 @@ int Engine::launch_call() {
             G6_CHECK(cudaMemcpyAsync(d_irec_, h_irec_, sizeof(IRec) * ni, cudaMemcpyHostToDevice, stream_),
                      "i copy");
             stats_.h2d_bytes += (long long)sizeof(IRec) * ni;
+            if (call_g4_) {
+                G6_CHECK(cudaMemcpyAsync(d_ieps2_, h_ieps2_, sizeof(double) * ni, cudaMemcpyHostToDevice, stream_),
+                         "i copy");
+                stats_.h2d_bytes += (long long)sizeof(double) * ni;
+            }
         }
         ForceConfig cfg = override_.il > 0 ? override_ : choose_config(km, ni, nj_pad, num_sms_, call_nb_);
         if (ensure_call_buffers(ni, call_nb_, partial_bytes(cfg, ni))) return -1;
@@ -473,9 +502,11 @@ int Engine::launch_call() {
         p.include_self = npipes_ > 48;
         p.status = status;
         p.tile_counter = d_tile_cnt_;
+        p.ieps2 = call_g4_ ? d_ieps2_ : nullptr;
         if (call_nb_) G6_CHECK(cudaMemsetAsync(d_nb_count_, 0, sizeof(int) * ni, stream_), "memset");
         if (timed_) G6_CHECK(cudaEventRecord(ev_force0_, stream_), "event");
-        G6_CHECK(launch_force(stream_, km, cfg, p, n_nonident_ == 0, call_nb_), "force launch");
+        G6_CHECK(launch_force(stream_, km, cfg, p, n_nonident_ == 0 && !call_g4_, call_nb_, call_g4_),
+                 "force launch");
         if (timed_) G6_CHECK(cudaEventRecord(ev_force1_, stream_), "event");
         stats_.launches += 1;
         if (call_nb_) {
@@ -586,6 +617,7 @@ int Engine::sweep(int nj, int i0, int ni, double eps2, bool copy_out, double (*a
     call_nj_ = nj;
     call_eps2_ = eps2;
     call_nb_ = false;
+    call_g4_ = false;
     call_sweep_ = true;
     call_copy_ = copy_out;
     call_i0_ = i0;
@@ -673,6 +705,44 @@ int Engine::read_neighbours() {
     for (int i = 0; i < call_ni_; ++i)
         if (h_nb_count_[i] > nb_cap_) return 1;
     return 0;
+}
+
+int Engine::neighbour_count(int pipe) const {
+    if (!nb_read_ || pipe < 0 || pipe >= call_ni_) return -1;
+    return call_nb_ ? h_nb_count_[pipe] : 0;
+}
+
+int Engine::neighbours_all(int pipe, int *nbl) {
+    const int count = neighbour_count(pipe);
+    if (count <= 0) return count;
+    if (count <= nb_cap_) {
+        memcpy(nbl, nb_host_.data() + h_nb_off_[pipe], sizeof(int) * count);
+        return count;
+    }
+    if (!call_g4_ || kmode() != kKernF64) {
+        last_error = "g6b200: full neighbour lists need a GRAPE-4 call";
+        return -1;
+    }
+    // Longer than the force kernel's per-i capacity: one pass over the
+    // predicted j-set (still in d_jrec_) for this pipe alone.
+    G6_CHECK(cudaSetDevice(device_), "cudaSetDevice");
+    int *d_buf = nullptr;
+    G6_CHECK(cudaMalloc(&d_buf, sizeof(int) * ((size_t)count + 1)), "nb full");
+    cudaError_t e = launch_nb_full_g4(stream_, d_jrec_, call_nj_, h_irec_[pipe], h_ieps2_[pipe], d_buf + 1, count,
+                                      d_buf);
+    int got = -1;
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&got, d_buf, sizeof(int), cudaMemcpyDeviceToHost, stream_);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(nbl, d_buf + 1, sizeof(int) * count, cudaMemcpyDeviceToHost, stream_);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(stream_);
+    cudaFree(d_buf);
+    if (e != cudaSuccess) return fail("nb full", e);
+    stats_.launches++;
+    stats_.d2h_bytes += 4LL * (count + 1);
+    if (got != count) {
+        last_error = "g6b200: full neighbour pass disagrees with the force kernel's count";
+        return -1;
+    }
+    return count;
 }
 
 int Engine::get_neighbours(int pipe, int max_length, int *nblen, int *nbl) {

@@ -47,6 +47,13 @@ class Engine {
 
     int firsthalf(int nj, int ni, const int *index, const double (*xi)[3],
                   const double (*vi)[3], double eps2, const double *h2);
+    // GRAPE-4 pipeline (FP64 mode only): per-i softening eps2[i], pairs
+    // with softened r2 == 0 skipped instead of an index exclusion, neighbour
+    // test on the softened r2 (src/harpsims/harp3fastsim.c:240-300).  The
+    // values are taken as the pipeline uses them (the GRAPE-4 ABI layer
+    // applies that simulator's factor 2).  Results come from lasthalf.
+    int firsthalf_g4(int nj, int ni, const double (*xi)[3], const double (*vi)[3], const double *eps2,
+                     const double *h2);
     int lasthalf(int ni, double (*acc)[3], double (*jerk)[3], double *pot, int *nn);
     // Self-gravity sweep: forces on the j-addresses [i0, i0+ni) themselves,
     // predicted on the device (no host i-arrays).  Blocking.  With
@@ -55,6 +62,13 @@ class Engine {
               double *pot, int *nn);
     int read_neighbours();
     int get_neighbours(int pipe, int max_length, int *nblen, int *nbl);
+    // Neighbour count of a pipe of the last call (after read_neighbours).
+    int neighbour_count(int pipe) const;
+    // The whole ascending list of a pipe of the last GRAPE-4 call, however
+    // long (lists beyond the per-i capacity are recomputed for that pipe on
+    // the device).  nbl has room for neighbour_count(pipe) entries.
+    // Returns the count, or -1.
+    int neighbours_all(int pipe, int *nbl);
 
     // For batched launches (server): flush staged j updates, widen the
     // fixed-point range for xi, predict j to the current ti if stale -- all
@@ -85,6 +99,8 @@ class Engine {
   private:
     int ensure_capacity(int address);
     int ensure_call_buffers(int ni, bool nb, size_t part_bytes);
+    int firsthalf_impl(int nj, int ni, const int *index, const double (*xi)[3], const double (*vi)[3],
+                       double eps2, const double *ieps2, const double *h2);
     int ensure_nb_buffers();
     int launch_call();  // predictor (if stale) + force + nb compaction + D2H
     int wait_call();    // wait; handle the fixed-point range retry
@@ -135,6 +151,7 @@ class Engine {
     // per-call buffers
     int call_cap_ = 0;
     IRec *h_irec_ = nullptr, *d_irec_ = nullptr;
+    double *h_ieps2_ = nullptr, *d_ieps2_ = nullptr;  // GRAPE-4 per-i softening
     unsigned char *h_out_ = nullptr, *d_out_ = nullptr;
     size_t part_cap_ = 0;
     Partial *d_part_ = nullptr;
@@ -155,6 +172,7 @@ class Engine {
     int call_ni_ = 0, call_nj_ = 0;
     double call_eps2_ = 0;
     bool call_nb_ = false;
+    bool call_g4_ = false;
     bool call_error_ = false;
     bool call_sweep_ = false;
     bool call_copy_ = true;

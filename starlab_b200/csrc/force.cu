@@ -7,6 +7,12 @@
 // self excluded by index; the nearest neighbour is the first address with
 // the smallest dr.dr (no softening; hdyn_inline.C:34-77).
 //
+// GRAPE-4 variant (FP64 only, kVarG4): the pipeline of the reference's
+// GRAPE-4 simulator (src/harpsims/harp3fastsim.c:240-300): per-i softening,
+// r2 = dr.dr + eps2_i; a pair contributes only when r2 > 0 (no exclusion by
+// index: kira stores the block's own particles at the block time, so self
+// has dr = 0 exactly); neighbour test r2 < h2_i on the softened r2.
+//
 // Work decomposition (one launch):
 //   gridDim.x  i-tiles;  gridDim.y  j-splits (contiguous address ranges,
 //              whole tiles; their partial sums are reduced in split order by
@@ -82,6 +88,7 @@ struct StateMixed : StateMixedBase {
 
 struct StateF64 {
     double x, y, z, vx, vy, vz, h2;
+    double eps2;  // per-i softening (GRAPE-4 variant only)
     double Ax, Ay, Az, Jx, Jy, Jz, Pt;
     double nr2;
     int nj, idx, i;
@@ -190,7 +197,7 @@ __device__ __forceinline__ void interact_mixed(S &s, const JMixed &J, int jg, fl
     }
 }
 
-template <bool CHK, bool NB, bool IDENT>
+template <bool CHK, bool NB, bool IDENT, bool G4 = false>
 __device__ __forceinline__ void interact(StateF64 &s, const double4 &pos, const double4 &vel,
                                          int jg, double eps2, const ForceParams &p) {
     const double dx = pos.x - s.x;
@@ -199,8 +206,34 @@ __device__ __forceinline__ void interact(StateF64 &s, const double4 &pos, const 
     const double dvx = vel.x - s.vx;
     const double dvy = vel.y - s.vy;
     const double dvz = vel.z - s.vz;
-    const double r2n = dx * dx + dy * dy + dz * dz;
     const double rv = dx * dvx + dy * dvy + dz * dvz;
+    if (G4) {
+        // The same rounding sequence as g4_r2() in the neighbour-list pass.
+        double r2 = g4_r2(dx, dy, dz, s.eps2);
+        if (NB && r2 < s.h2) nb_push(p, s.i, jg);
+        const bool zero = !(r2 > 0.0);
+        const double mj = zero ? 0.0 : pos.w;
+        const double r2nn = zero ? DBL_MAX : r2;
+        r2 = zero ? 1.0 : r2;
+        const double rinv = rsqrt(r2);
+        const double r2inv = rinv * rinv;
+        const double mr = mj * rinv;
+        const double mr3 = mr * r2inv;
+        const double a3 = -3.0 * rv * r2inv;
+        s.Pt -= mr;
+        s.Ax += mr3 * dx;
+        s.Ay += mr3 * dy;
+        s.Az += mr3 * dz;
+        s.Jx += mr3 * (dvx + a3 * dx);
+        s.Jy += mr3 * (dvy + a3 * dy);
+        s.Jz += mr3 * (dvz + a3 * dz);
+        if (r2nn < s.nr2) {
+            s.nr2 = r2nn;
+            s.nj = jg;
+        }
+        return;
+    }
+    const double r2n = dx * dx + dy * dy + dz * dz;
     double r2 = r2n + eps2;
     double mj = pos.w;
     double r2nn = r2n;
@@ -355,6 +388,8 @@ __device__ __forceinline__ void fold(StateMixedBase &s) {
 // 2).  Unrolling by 4 measured 1.3% faster for the scalar layout and equal
 // for the paired one.
 constexpr int kVarUnroll4 = 2;
+// 4 = GRAPE-4 pipeline (FP64 kernel only; see the file header).
+constexpr int kVarG4 = 4;
 
 // Consume one shared-memory tile: this thread's j are kbase + m*JL.
 template <int K, int R, int JL, bool CHK, bool NB, bool IDENT, int V>
@@ -394,7 +429,8 @@ __device__ __forceinline__ void consume_tile(typename StateOf<K>::type (&st)[R],
             const double4 pos = S[k].pos;
             const double4 vel = S[k].vel;
 #pragma unroll
-            for (int r = 0; r < R; ++r) interact<CHK, NB, IDENT>(st[r], pos, vel, tb + k, eps2, p);
+            for (int r = 0; r < R; ++r)
+                interact<CHK, NB, IDENT, (V & kVarG4) != 0>(st[r], pos, vel, tb + k, eps2, p);
         }
     } else {
         const float eps2 = (float)p.eps2;
@@ -556,6 +592,7 @@ __device__ __forceinline__ void process_task(const ForceParams &p, int itile_idx
         const int i = i0 + r * IL;
         const bool valid = i < p.ni;
         load_i(st[r], p.irec[valid ? i : p.ni - 1], p, range_ok);
+        if constexpr (K == kKernF64 && (V & kVarG4) != 0) st[r].eps2 = p.ieps2[valid ? i : p.ni - 1];
         st[r].i = i;
         if (!valid) st[r].h2 = 0;
     }
@@ -756,6 +793,15 @@ static KernelFn pick2(int il, int r, bool nb, bool ident) {
     return pick3<K, 1, 1>(nb, ident);
 }
 
+// GRAPE-4 pipeline: FP64 layout, no index identity.
+static KernelFn pick_g4(int il, int r, bool nb) {
+    constexpr int K = kKernF64, V = kVarG4;
+    if (il == 32 && r == 2) return nb ? force_kernel<K, 32, 2, true, false, V> : force_kernel<K, 32, 2, false, false, V>;
+    if (il == 32) return nb ? force_kernel<K, 32, 1, true, false, V> : force_kernel<K, 32, 1, false, false, V>;
+    if (il == 8) return nb ? force_kernel<K, 8, 1, true, false, V> : force_kernel<K, 8, 1, false, false, V>;
+    return nb ? force_kernel<K, 1, 1, true, false, V> : force_kernel<K, 1, 1, false, false, V>;
+}
+
 static KernelFn pick(int kmode, int il, int r, bool nb, bool ident) {
     if (kmode == kKernMixedP) return pick2<kKernMixedP>(il, r, nb, ident);
     if (kmode == kKernMixedDS) return pick2<kKernMixedDS>(il, r, nb, ident);
@@ -870,7 +916,8 @@ cudaError_t launch_force_batch(cudaStream_t s, int kmode, const ForceConfig &cfg
 }
 
 cudaError_t launch_force(cudaStream_t s, int kmode, const ForceConfig &cfg, ForceParams p,
-                         bool ident, bool nb) {
+                         bool ident, bool nb, bool g4) {
+    if (g4 && (kmode != kKernF64 || !p.ieps2)) return cudaErrorInvalidValue;
     const int T = tile_size(kmode);
     const int ntiles = p.nj_pad / T;
     if (p.ni <= 0) return cudaSuccess;
@@ -887,7 +934,7 @@ cudaError_t launch_force(cudaStream_t s, int kmode, const ForceConfig &cfg, Forc
     const int itile = G * cfg.il * cfg.r;
     dim3 grid((p.ni + itile - 1) / itile, p.nsplit);
     dim3 block(32 * cfg.warps);
-    KernelFn fn = pick(kmode, cfg.il, cfg.r, nb, ident);
+    KernelFn fn = g4 ? pick_g4(cfg.il, cfg.r, nb) : pick(kmode, cfg.il, cfg.r, nb, ident);
     size_t sm = smem_bytes(kmode, cfg);
     fn<<<grid, block, sm, s>>>(p);
     cudaError_t e = cudaGetLastError();

@@ -61,6 +61,11 @@ struct ForceParams {
     // order and writes the results, so no separate reduction launch is needed;
     // it leaves its counter at zero again.
     int *tile_counter;
+    // GRAPE-4 calls only (null otherwise): per-i softening eps2_i.  With it
+    // the kernel follows the GRAPE-4 pipeline: r2 = dr.dr + eps2_i, pairs
+    // with r2 == 0 contribute nothing (no exclusion by index), and the
+    // neighbour test is r2 < h2_i on the softened r2.
+    const double *ieps2;
 };
 
 // A batch of calls for the persistent multi-item kernel (device pointers).
@@ -98,7 +103,7 @@ size_t jrec_bytes(int kmode);
 ForceConfig choose_config(int kmode, int ni, int nj_pad, int num_sms, bool nb);
 // Launch force (+ split reduction).  Returns a cudaError_t.
 cudaError_t launch_force(cudaStream_t s, int kmode, const ForceConfig &cfg, ForceParams p,
-                         bool ident, bool nb);
+                         bool ident, bool nb, bool g4 = false);
 size_t partial_bytes(const ForceConfig &cfg, int ni);
 
 // Batched launches.  batch_plan fills jper/nsplit/H of one item from its own
@@ -157,5 +162,9 @@ int batch_ctas(int kmode, const ForceConfig &cfg, int num_sms);
 // offsets[ni+1] (exclusive scan of min(count, cap)), out[total].
 cudaError_t launch_nb_compact(cudaStream_t s, int ni, const int *count, const int *list, int cap,
                               long long *offsets, int *out);
+// Full ascending neighbour list of one GRAPE-4 i-record over the predicted
+// FP64 j-records (JRecF64[nj]); at most cap entries, *count = hits.
+cudaError_t launch_nb_full_g4(cudaStream_t s, const void *jrec, int nj, const IRec &q, double eps2, int *out,
+                              int cap, int *count);
 
 }  // namespace g6

@@ -77,6 +77,55 @@ __global__ void nb_sort_kernel(const int *__restrict__ count, const int *__restr
     for (int k = threadIdx.x; k < n; k += blockDim.x) dst[k] = keys[k];
 }
 
+// Full neighbour list of one GRAPE-4 i-particle over the predicted FP64
+// j-set, for lists longer than the per-i capacity of the force kernel's
+// lists (the GRAPE-4 readout h3nblist_ has no length limit).  One CTA of
+// 1024 threads walks the addresses in order; each chunk's hits are placed by
+// a ballot prefix, so the list comes out ascending.  The test is the force
+// kernel's (g4_r2 < h2_i).  Writes at most cap entries; *count gets the
+// number of hits.
+__global__ void __launch_bounds__(1024) nb_full_g4_kernel(const JRecF64 *__restrict__ jrec, int nj, IRec q,
+                                                          double eps2, int *__restrict__ out, int cap,
+                                                          int *__restrict__ count) {
+    __shared__ int warp_hits[32];
+    __shared__ int base;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int nw = blockDim.x >> 5;
+    if (threadIdx.x == 0) base = 0;
+    __syncthreads();
+    for (int j0 = 0; j0 < nj; j0 += blockDim.x) {
+        const int j = j0 + threadIdx.x;
+        bool hit = false;
+        if (j < nj) {
+            const double4 p = jrec[j].pos;
+            hit = g4_r2(p.x - q.x[0], p.y - q.x[1], p.z - q.x[2], eps2) < q.h2;
+        }
+        const unsigned b = __ballot_sync(0xffffffffu, hit);
+        if (lane == 0) warp_hits[w] = __popc(b);
+        __syncthreads();
+        int off = base;
+        for (int k = 0; k < w; ++k) off += warp_hits[k];
+        if (hit) {
+            const int pos = off + __popc(b & ((1u << lane) - 1u));
+            if (pos < cap) out[pos] = j;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            int t = 0;
+            for (int k = 0; k < nw; ++k) t += warp_hits[k];
+            base += t;
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *count = base;
+}
+
+cudaError_t launch_nb_full_g4(cudaStream_t s, const void *jrec, int nj, const IRec &q, double eps2, int *out,
+                              int cap, int *count) {
+    nb_full_g4_kernel<<<1, 1024, 0, s>>>(reinterpret_cast<const JRecF64 *>(jrec), nj, q, eps2, out, cap, count);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_nb_compact(cudaStream_t s, int ni, const int *count, const int *list, int cap,
                               long long *offsets, int *out) {
     if (ni <= 0) return cudaSuccess;

@@ -1,0 +1,280 @@
+"""GRAPE-4 ABI (libh3b200.so) parity on the GPU, through the C ABI.
+
+The engine runs the GRAPE-4 pipeline variant of the FP64 force kernel
+behind Starlab's h3* entry points (include/grape4.h:22-45).  It is checked
+against the oracle's restatement of the reference's GRAPE-4 simulator
+(oracle/g4_oracle.c, itself pinned bit for bit to
+src/harpsims/harp3fastsim.c by tests/test_g4_oracle.py) and against the
+committed fixtures made by that simulator:
+
+    acc, jerk, pot   per-particle relative error <= 1e-12 (FP64 mode)
+    neighbour lists  identical, except j whose softened r2 lies within 1e-9
+                     (relative) of 2 h2 (rounding at the sphere's edge)
+
+plus the ABI's own behaviour: DMA buffers with indirect host indices,
+deduplicated padding and USE_HALF_CHIP slot pairs, lists longer than the
+force pass keeps per i, the simulator's exit on oversized calls, and
+Starlab's own kira / hsys_stats driving the library (their GRAPE-4 branch,
+kira_config.C:65-95).
+"""
+import glob
+import os
+import re
+import subprocess
+import sys
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REPO = os.path.dirname(HERE)
+REF = os.path.join(REPO, "oracle", "_ref")
+GOLDEN = sorted(glob.glob(os.path.join(HERE, "golden", "g4_*.npz")))
+TOL = 1e-12
+EDGE = 1e-9
+
+
+@pytest.fixture(scope="module")
+def h3():
+    from starlab_b200.grape4 import H3Engine
+    eng = H3Engine()
+    yield eng
+
+
+@pytest.fixture(scope="module")
+def g4o():
+    from oracle.oracle import G4Oracle
+    return G4Oracle()
+
+
+def rel_vec(a, b):
+    nb = np.linalg.norm(b, axis=1)
+    return np.linalg.norm(a - b, axis=1) / np.where(nb > 0, nb, 1.0)
+
+
+def check_forces(got, want):
+    (a, j, p), (wa, wj, wp) = got, want
+    ea, ej = rel_vec(a, wa), rel_vec(j, wj)
+    ep = np.abs(p - wp) / np.abs(wp)
+    assert ea.max() <= TOL and ej.max() <= TOL and ep.max() <= TOL, (ea.max(), ej.max(), ep.max())
+
+
+def check_lists(h3, xp, xi, eps2, h2, want_lists, slots=None):
+    slots = range(len(want_lists)) if slots is None else slots
+    for k in slots:
+        got = h3.nblist(k)
+        want = want_lists[k]
+        if np.array_equal(got, want):
+            continue
+        diff = np.setxor1d(got, want)
+        r2 = 2 * eps2[k] + np.sum((xp[diff] - xi[k]) ** 2, axis=1)
+        assert np.all(np.abs(r2 - 2 * h2[k]) <= EDGE * 2 * h2[k]), (k, diff)
+
+
+def load_in_buffers(h3, g, nbuf=3):
+    """Store every j through h3mjpdma_indirect_ with permuted host indices,
+    spread over auto-numbered buffers, committed by h3mjpdma_flush_."""
+    n = g["x"].shape[0]
+    perm = np.random.default_rng(n).permutation(n) + 1
+    for part in np.array_split(perm, nbuf):
+        h3.mjpdma_indirect(part, g["x"], g["v"], g["aj"], g["jj"], g["m"], g["t"], buff_id=-1)
+    h3.mjpdma_flush()
+
+
+@pytest.mark.parametrize("path", GOLDEN, ids=[os.path.basename(p)[:-4] for p in GOLDEN])
+def test_simulator_fixtures(h3, g4o, path):
+    g = np.load(path)
+    n = g["x"].shape[0]
+    load_in_buffers(h3, g)
+    h3.setti(float(g["ti"]))
+    acc, jerk, pot = h3.calc(n, g["xi"], g["vi"], g["eps2"], g["h2"])
+    xp, vp = g4o.predict(float(g["ti"]), g["t"], g["x"], g["v"], g["aj"], g["jj"])
+    _, _, opot, _, _ = g4o.force(xp, vp, g["m"], g["xi"], g["vi"], g["eps2"], g["h2"])
+    check_forces((acc, jerk, pot), (g["acc"], g["jerk"], opot))
+    h3.nbread()
+    off, idx = g["nb_off"], g["nb_idx"]
+    want = [idx[off[i]:off[i + 1]] for i in range(len(off) - 1)]
+    check_lists(h3, xp, g["xi"], g["eps2"], g["h2"], want)
+
+
+def kira_like(n, nblock, seed, half_chip, npipe):
+    from starlab_b200 import ics
+    from oracle.oracle import G4Oracle
+    m, x, v = ics.plummer(n, seed)
+    rng = np.random.default_rng(seed)
+    aj = 0.5 * (-x / (1.0 + np.sum(x * x, axis=1, keepdims=True)) ** 1.5)
+    jj = rng.normal(scale=0.5, size=(n, 3)) / 6.0
+    t = rng.uniform(0.0, 1.0 / 64, n)
+    ti = 1.0 / 64
+    block = np.sort(rng.choice(n, nblock, replace=False))
+    xp, vp = G4Oracle().predict(ti, t, x, v, aj, jj)
+    x, v, t = x.copy(), v.copy(), t.copy()
+    x[block], v[block], t[block] = xp[block], vp[block], ti
+    h2 = np.full(nblock, (0.5 / n ** (1 / 3)) ** 2)
+    h2[::3] = 0.0
+    xi, vi, e2 = x[block], v[block], np.zeros(nblock)
+    hi = h2
+    if half_chip:
+        xi, vi, e2, hi = (np.repeat(a, 2, axis=0) for a in (xi, vi, e2, hi))
+    pad = npipe - xi.shape[0]
+    xi, vi, e2, hi = (np.concatenate([a, np.repeat(a[-1:], pad, axis=0)]) for a in (xi, vi, e2, hi))
+    return dict(m=m, x=x, v=v, aj=aj, jj=jj, t=t, ti=ti, xi=xi, vi=vi, eps2=e2, h2=hi, nblock=nblock)
+
+
+@pytest.mark.parametrize("half_chip", [False, True])
+def test_kira_style_block_padded_to_npipe(h3, g4o, half_chip):
+    """A 20000-body system, a block of 1500 stored at the block time, the
+    slots padded to h3npipe_() as force_by_grape4 does (hdyn_grape4.C:
+    350-382): every slot agrees with the oracle, padding and pair slots are
+    computed once."""
+    npipe = h3.npipe()
+    d = kira_like(20000, 1500, 5 + half_chip, half_chip, npipe)
+    n = d["x"].shape[0]
+    h3.set_j_particles(d["x"], d["v"], d["aj"], d["jj"], d["m"], d["t"])
+    h3.setti(d["ti"])
+    s0 = h3.stats()
+    acc, jerk, pot = h3.calc(n, d["xi"], d["vi"], d["eps2"], d["h2"])
+    s1 = h3.stats()
+    assert s1["slots"] - s0["slots"] == npipe
+    assert s1["computed"] - s0["computed"] == d["nblock"]
+    xp, vp = g4o.predict(d["ti"], d["t"], d["x"], d["v"], d["aj"], d["jj"])
+    step = 2 if half_chip else 1
+    used = np.arange(0, d["nblock"] * step)
+    oa, oj, op, cnt, nb = g4o.force(xp, vp, d["m"], d["xi"][used], d["vi"][used], d["eps2"][used], d["h2"][used])
+    check_forces((acc[used], jerk[used], pot[used]), (oa, oj, op))
+    # padding slots repeat the last real slot bit for bit
+    last = used[-1]
+    assert np.array_equal(acc[last:], np.repeat(acc[last:last + 1], npipe - last, axis=0))
+    h3.nbread()
+    check_lists(h3, xp, d["xi"][used], d["eps2"][used], d["h2"][used], nb)
+    # self is listed when h2 > 0 (kira needs >= 2 entries to see a neighbour)
+    for k in range(0, len(used), step * 7):
+        self_j = np.flatnonzero(np.all(xp == d["xi"][k], axis=1))
+        assert (self_j[0] in h3.nblist(k)) == (d["h2"][k] > 0)
+
+
+def test_lists_longer_than_the_per_i_capacity(h3, g4o):
+    """h3nblist_ has no length argument: lists beyond the force pass's
+    per-i capacity (4096) come back whole and ascending."""
+    from starlab_b200 import ics
+    n = 12000
+    m, x, v = ics.plummer(n, 9)
+    z = np.zeros((n, 3))
+    h3.set_j_particles(x, v, z, z, m, 0.0)
+    h3.setti(0.0)
+    xi = np.array([[0.0, 0.0, 0.0], [0.3, 0.1, -0.2], [2.0, 2.0, 2.0]])
+    vi = np.zeros((3, 3))
+    h2 = np.array([1.0, 0.4, 1e-4])
+    acc, jerk, pot = h3.calc(n, xi, vi, 1e-6, h2)
+    xp, vp = x, v
+    oa, oj, op, cnt, nb = g4o.force(xp, vp, m, xi, vi, 1e-6, h2)
+    check_forces((acc, jerk, pot), (oa, oj, op))
+    h3.nbread()
+    assert cnt[0] > 4096 and cnt[1] > 4096
+    for k in range(3):
+        got = h3.nblist(k)
+        r2 = 2e-6 + np.sum((xp - xi[k]) ** 2, axis=1)
+        at_edge = np.sum(np.abs(r2 - 2 * h2[k]) <= EDGE * 2 * h2[k])
+        assert abs(got.size - cnt[k]) <= at_edge
+        assert np.all(np.diff(got) > 0)
+    check_lists(h3, xp, xi, np.full(3, 1e-6), h2, nb)
+
+
+def test_buffer_order_and_updates(h3, g4o):
+    """Later commits to the same address win, as in the simulator's
+    h3mjpdma_start_ (harp3fastsim.c:182-206); results follow the updates."""
+    from starlab_b200 import ics
+    n = 3000
+    m, x, v = ics.plummer(n, 17)
+    z = np.zeros((n, 3))
+    h3.set_j_particles(x, v, z, z, m, 0.0)
+    x2 = x.copy()
+    x2[:100] += 0.01
+    h3.mjpdma_indirect(np.arange(1, 101), x2, v, z, z, m, np.zeros(n), buff_id=4)
+    x3 = x2.copy()
+    x3[50:100] -= 0.02
+    h3.mjpdma_indirect(np.arange(51, 101), x3, v, z, z, m, np.zeros(n), buff_id=5)
+    h3.mjpdma_start(4)
+    h3.mjpdma_start(5)
+    h3.setti(0.0)
+    xi, vi = x3[:256], v[:256]
+    got = h3.calc(n, xi, vi, 1e-5, 0.0)
+    oa, oj, op, _, _ = g4o.force(x3, v, m, xi, vi, 1e-5, 0.0)
+    check_forces(got, (oa, oj, op))
+
+
+def _run_py(code, env=None):
+    e = dict(os.environ)
+    e.update(env or {})
+    return subprocess.run([sys.executable, "-c", code], cwd=REPO, env=e, stdout=subprocess.PIPE,
+                          stderr=subprocess.PIPE, text=True, timeout=300)
+
+
+def test_oversized_calls_exit_like_the_simulator():
+    """The simulator prints and exit(-1)s on ni above its pipes or an
+    oversized DMA (harp3fastsim.c:155-158, 232-236); so does the library,
+    before touching the device."""
+    pre = ("import numpy as np, sys; sys.path.insert(0, '.');"
+           "from starlab_b200.grape4 import H3Engine; h=H3Engine();")
+    r = _run_py(pre + "n=h.npipe()+1; h.calc(10, np.zeros((n,3)), np.zeros((n,3)), 0.0, 0.0)",
+                {"H3B200_NPIPES": "64"})
+    assert r.returncode == 255 and "Too large ni (65 > 64)" in r.stderr, (r.returncode, r.stderr[-500:])
+
+
+def _need(name):
+    p = os.path.join(REF, name)
+    if not os.path.exists(p):
+        pytest.skip("%s not built (python oracle/build_ref.py on a machine with the reference)" % name)
+    return p
+
+
+def _energies(log):
+    return [float(m.group(1)) for m in re.finditer(r"Energies:\s+\S+\s+\S+\s+(\S+)", log)]
+
+
+@pytest.fixture(scope="module")
+def plummer1024(tmp_path_factory):
+    mk = _need("makeplummer")
+    d = tmp_path_factory.mktemp("kira4")
+    snap = os.path.join(d, "p1024.snap")
+    with open(snap, "w") as f:
+        subprocess.run([mk, "-n", "1024", "-s", "42", "-i"], stdout=f, stderr=subprocess.DEVNULL, check=True)
+    return str(d), snap
+
+
+def _run(exe, args, snap, cwd):
+    with open(snap) as fin:
+        r = subprocess.run([exe] + args, stdin=fin, stdout=subprocess.PIPE, stderr=subprocess.PIPE,
+                           timeout=900, cwd=cwd, text=True)
+    assert r.returncode == 0, r.stderr[-3000:]
+    return r.stderr
+
+
+def test_hsys_stats_energy_through_grape4(plummer1024):
+    """grape4_calculate_energies (hdyn_grape4.C:789-840): the potential
+    returned through the ABI gives the CPU tool's energy."""
+    d, snap = plummer1024
+    cpu = _energies(_run(_need("hsys_stats"), [], snap, d))
+    g4 = _run(_need("hsys_stats_g4"), [], snap, d)
+    assert "GRAPE-4" in g4
+    e4 = _energies(g4)
+    assert cpu and e4 and e4[0] == pytest.approx(cpu[0], rel=1e-12)
+
+
+def test_kira_grape4_energy_within_2x_of_cpu(plummer1024):
+    """Starlab's kira, GRAPE-4 branch (built with USE_HALF_CHIP as configure
+    does for a GRAPE-4 library), N = 1024 Plummer to t = 1: the energy error
+    stays within 2x of the CPU run's."""
+    d, snap = plummer1024
+    args = ["-t", "1", "-d", "0.25", "-e", "0.001", "-a", "0.02"]
+    cpu = _energies(_run(_need("kira"), ["-0"] + args, snap, d))
+    g4 = _run(_need("kira_g4"), args, snap, d)
+    assert "GRAPE-4" in g4, g4[:2000]
+    e4 = _energies(g4)
+    assert len(cpu) >= 5 and len(e4) >= 5
+    de_cpu = max(abs(e - cpu[0]) for e in cpu[1:])
+    de_g4 = max(abs(e - e4[0]) for e in e4[1:])
+    assert e4[0] == pytest.approx(cpu[0], rel=1e-12)
+    assert de_g4 <= 2.0 * de_cpu, (de_g4, de_cpu)
