@@ -29,7 +29,10 @@ with g++ directly (no autotools: they are absent here), into ``oracle/_ref/``:
 * ``kira_g4``/``hsys_stats_g4``  the mains linked against ``libh3b200.so``,
                        with ``hdyn_grape4.C`` recompiled under
                        ``USE_HALF_CHIP`` as configure defines it when it finds
-                       a GRAPE-4 library (``configure.ac:216-222``).
+                       a GRAPE-4 library (``configure.ac:216-222``);
+* ``kira_g4o``/``hsys_stats_g4o``  the same GRAPE-4 branch on the CPU, over
+                       ``oracle/h3_oracle.c`` + ``oracle/g4_oracle.c`` (the
+                       GRAPE-4 ABI on the oracle's pipeline restatement).
 
 Nothing here is shipped; the outputs are git-ignored.  Usage:
 ``python oracle/build_ref.py [--jobs N] [--ref PATH]``.
@@ -160,6 +163,11 @@ def main():
     add(os.path.join(HERE, "ref_force.C"), harness_obj)
     g4_obj = os.path.join(OUT, "obj", "hdyn_grape4_half_chip.o")
     add(os.path.join(src, "node/dyn/hdyn/evolve/hdyn_grape4.C"), g4_obj, extra=["-DUSE_HALF_CHIP=1"])
+    h3o_objs = []
+    for f in ("h3_oracle.c", "g4_oracle.c"):
+        obj = os.path.join(OUT, "obj", "oracle__" + f + ".o")
+        add(os.path.join(HERE, f), obj, extra=["-ffp-contract=off"], c=True)
+        h3o_objs.append(obj)
     sim_src = os.path.join(src, "harpsims", "harp3fastsim.c")
     sim_obj = os.path.join(OUT, "obj", "harp3fastsim.o")
     add(sim_src, sim_obj, extra=["-std=gnu89"], c=True)
@@ -194,6 +202,12 @@ def main():
     sim_so = os.path.join(OUT, "libharp3sim.so")
     if not up_to_date(sim_so, [sim_obj]):
         run(["gcc", "-shared", "-o", sim_so, sim_obj, "-lm"])
+
+    # kira and hsys_stats, GRAPE-4 branch, over the CPU oracle pipeline.
+    for name in ("kira", "hsys_stats"):
+        exe = os.path.join(OUT, name + "_g4o")
+        if not up_to_date(exe, [tool_objs[name], g4_obj, lib, stubs] + h3o_objs):
+            run(["g++", "-o", exe, tool_objs[name], g4_obj, lib] + h3o_objs + [stubs] + link_tail)
 
     # kira and hsys_stats driving the GPU engine through the unchanged g6 ABI.
     g6lib_dir = os.path.join(REPO, "starlab_b200", "lib")

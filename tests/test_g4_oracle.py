@@ -154,3 +154,35 @@ def test_h3_npipe_without_device():
     env = dict(os.environ, H3B200_NPIPES="96")
     r = subprocess.run([sys.executable, "-c", code, LIB_PATH], env=env, stdout=subprocess.PIPE, text=True)
     assert r.stdout.split() == ["96", "1048576", "1"]
+
+
+def test_kira_grape4_branch_on_the_oracle_pipeline(tmp_path):
+    """Starlab's kira, GRAPE-4 branch, over the oracle's CPU pipeline
+    (oracle/h3_oracle.c): the integration the GPU library is compared
+    with.  The branch computes without softening (hdyn_grape4.C:320-330), so
+    the initial energy is the unsoftened Plummer value, -1/4; its energy
+    error over t = 0.5 stays within 2x of kira -0's."""
+    import re
+    ref = os.path.join(REPO, "oracle", "_ref")
+    exes = [os.path.join(ref, n) for n in ("makeplummer", "kira", "kira_g4o")]
+    if not all(os.path.exists(e) for e in exes):
+        pytest.skip("oracle/_ref not built (reference tree absent)")
+    snap = tmp_path / "p.snap"
+    with open(snap, "w") as f:
+        subprocess.run([exes[0], "-n", "512", "-s", "42", "-i"], stdout=f, stderr=subprocess.DEVNULL, check=True)
+    args = ["-t", "0.5", "-d", "0.125", "-e", "0.001", "-a", "0.02"]
+
+    def energies(cmd):
+        with open(snap) as fin:
+            r = subprocess.run(cmd, stdin=fin, stdout=subprocess.DEVNULL, stderr=subprocess.PIPE, text=True,
+                               timeout=300, cwd=tmp_path)
+        assert r.returncode == 0, r.stderr[-2000:]
+        return r.stderr, [float(m.group(1)) for m in re.finditer(r"Energies:\s+\S+\s+\S+\s+(\S+)", r.stderr)]
+
+    log, e4 = energies([exes[2]] + args)
+    _, e0 = energies([exes[1], "-0"] + args)
+    assert "found GRAPE-4 acceleration" in log
+    assert len(e4) >= 4 and e4[0] == pytest.approx(-0.25, abs=1e-14)
+    de4 = max(abs(e - e4[0]) for e in e4[1:])
+    de0 = max(abs(e - e0[0]) for e in e0[1:])
+    assert de4 <= 2.0 * de0, (de4, de0)
