@@ -41,7 +41,7 @@ def j_state(n, seed, salpeter=False):
 
 
 def kira_block(seed, n=600, nblock=40, half_chip=False, npipe=None):
-    """Block members re-stored at ti = the block time (hdyn_grape4.C:1203-1208)."""
+    """Block members re-stored at ti = the block time (hdyn_grape4.C:1203-1222)."""
     m, x, v, aj, jj, t = j_state(n, seed)
     ti = 0.0125
     rng = np.random.default_rng(seed)
