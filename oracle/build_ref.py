@@ -72,6 +72,8 @@ TOOLS = {
     "scale": "node/dyn/util/scale.C",
     "hsys_stats": "node/dyn/hdyn/util/hsys_stats.C",
     "hscale": "node/dyn/hdyn/util/hscale.C",
+    "get_densities": "node/dyn/hdyn/util/get_densities.C",
+    "compute_density": "node/dyn/util/compute_density.C",
 }
 CONFIG_H = """/* hand-written stand-in for the autoconf config.h of Starlab 4.4.4 */
 #define HAVE_LIBPTHREAD 1
@@ -204,7 +206,7 @@ def main():
         run(["gcc", "-shared", "-o", sim_so, sim_obj, "-lm"])
 
     # kira and hsys_stats, GRAPE-4 branch, over the CPU oracle pipeline.
-    for name in ("kira", "hsys_stats"):
+    for name in ("kira", "hsys_stats", "get_densities"):
         exe = os.path.join(OUT, name + "_g4o")
         if not up_to_date(exe, [tool_objs[name], g4_obj, lib, stubs] + h3o_objs):
             run(["g++", "-o", exe, tool_objs[name], g4_obj, lib] + h3o_objs + [stubs] + link_tail)
@@ -214,7 +216,7 @@ def main():
     g6lib = os.path.join(g6lib_dir, "libg6b200.so")
     if os.path.exists(g6lib):
         rpath = "-Wl,-rpath,$ORIGIN/../../starlab_b200/lib"
-        for name in ("kira", "hsys_stats", "hscale"):
+        for name in ("kira", "hsys_stats", "hscale", "get_densities"):
             exe = os.path.join(OUT, name + "_g6")
             if not up_to_date(exe, [tool_objs[name], lib, stubs, g6lib]):
                 run(["g++", "-o", exe, tool_objs[name], lib, "-L" + g6lib_dir, "-lg6b200",
@@ -223,7 +225,7 @@ def main():
     h3lib = os.path.join(g6lib_dir, "libh3b200.so")
     if os.path.exists(h3lib):
         rpath = "-Wl,-rpath,$ORIGIN/../../starlab_b200/lib"
-        for name in ("kira", "hsys_stats", "hscale"):
+        for name in ("kira", "hsys_stats", "hscale", "get_densities"):
             exe = os.path.join(OUT, name + "_g4")
             if not up_to_date(exe, [tool_objs[name], g4_obj, lib, stubs, h3lib]):
                 run(["g++", "-o", exe, tool_objs[name], g4_obj, lib, "-L" + g6lib_dir, "-lh3b200",
