@@ -27,6 +27,10 @@ Reported (one JSON line on rank 0):
                bounded sample of i
   latency      p50/p99 of single force calls through the C ABI, ni drawn
                from a power law (slope -1) on [1, N]
+  grape4       the GRAPE-4 ABI (libh3b200.so, FP64): a full sweep of an
+               N = 65536 Plummer sphere through h3calc_ in h3npipe_() chunks,
+               the block stored at the block time as kira's GRAPE-4 branch
+               does; wall-clock interactions/s through the ABI
 
 Multi-GPU (torchrun, one rank per GPU): every rank integrates its own
 independent cluster (different seed) -- weak scaling, no collective on the
@@ -66,6 +70,7 @@ def parse():
     ap.add_argument("--no-served", action="store_true")
     ap.add_argument("--ensemble-clusters", type=int, default=256)
     ap.add_argument("--ensemble-t", type=float, default=1.0)
+    ap.add_argument("--no-grape4", action="store_true")
     return ap.parse_args()
 
 
@@ -216,6 +221,35 @@ def served_section(seed):
             "one_call_at_a_time": {"p50_ms": float(np.percentile(lat2, 50) * 1e3),
                                    "p99_ms": float(np.percentile(lat2, 99) * 1e3),
                                    "interactions_per_s": inter2 / wall2}}
+
+
+def grape4_section(seed, n=65536, sweeps=3):
+    from starlab_b200 import ics
+    from starlab_b200.grape4 import H3Engine
+    m, x, v = ics.plummer(n, seed)
+    z = np.zeros((n, 3))
+    h3 = H3Engine()
+    npipe = h3.npipe()
+    h3.set_j_particles(x, v, z, z, m, 0.0)
+    h3.setti(0.0)
+
+    def sweep():
+        for i0 in range(0, n, npipe):
+            h3.calc(n, x[i0:i0 + npipe], v[i0:i0 + npipe], 0.0, 0.0)
+
+    sweep()
+    s0 = h3.stats()
+    t0 = time.perf_counter()
+    for _ in range(sweeps):
+        sweep()
+    sec = (time.perf_counter() - t0) / sweeps
+    s1 = h3.stats()
+    h3.close()
+    inter = n * (n - 1)
+    return {"n": n, "npipe": npipe, "precision": "fp64", "ms_per_sweep": sec * 1e3,
+            "interactions_per_s": inter / sec, "calls_per_sweep": (s1["calls"] - s0["calls"]) // sweeps,
+            "launches_per_sweep": (s1["launches"] - s0["launches"]) // sweeps,
+            "path": "h3mjpdma_indirect_/h3calc_ (host buffers, wall clock)"}
 
 
 def _rel(a, b):
@@ -436,6 +470,8 @@ def main():
             line["ensemble"] = ensemble_section(args.ensemble_clusters, args.ensemble_t, 2024)
         if dist.world == 1 and not args.no_served:
             line["served_stream"] = served_section(5)
+        if dist.world == 1 and not args.no_grape4:
+            line["grape4"] = grape4_section(7)
         if dist.world == 1 and not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(n, seed, os.cpu_count() or 1, gpu=(acc, jerk, pot, nn))
         print(json.dumps(line), flush=True)
