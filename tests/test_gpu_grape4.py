@@ -281,8 +281,12 @@ def test_kira_grape4_energy_within_2x_of_cpu(plummer1024):
     kira -0 (softened) is printed beside it."""
     d, snap = plummer1024
     args = ["-t", "1", "-d", "0.25", "-e", "0.001", "-a", "0.02"]
+    import time
+    t0 = time.perf_counter()
     cpu = _energies(_run(_need("kira_g4o"), args, snap, d))
+    t1 = time.perf_counter()
     g4 = _run(_need("kira_g4"), args, snap, d)
+    t2 = time.perf_counter()
     assert "GRAPE-4" in g4, g4[:2000]
     e4 = _energies(g4)
     soft = _energies(_run(_need("kira"), ["-0"] + args, snap, d))
@@ -290,6 +294,7 @@ def test_kira_grape4_energy_within_2x_of_cpu(plummer1024):
     de_cpu = max(abs(e - cpu[0]) for e in cpu[1:])
     de_g4 = max(abs(e - e4[0]) for e in e4[1:])
     de_soft = max(abs(e - soft[0]) for e in soft[1:])
-    print("kira GRAPE-4 |dE|: gpu %.3e  cpu-oracle %.3e  (kira -0 softened %.3e)" % (de_g4, de_cpu, de_soft))
+    print("kira GRAPE-4 |dE|: gpu %.3e  cpu-oracle %.3e  (kira -0 softened %.3e); wall: gpu %.1f s, cpu-oracle %.1f s"
+          % (de_g4, de_cpu, de_soft, t2 - t1, t1 - t0))
     assert e4[0] == pytest.approx(cpu[0], rel=1e-12)
     assert de_g4 <= 2.0 * de_cpu, (de_g4, de_cpu)
