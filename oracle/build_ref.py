@@ -32,7 +32,10 @@ with g++ directly (no autotools: they are absent here), into ``oracle/_ref/``:
                        a GRAPE-4 library (``configure.ac:216-222``);
 * ``kira_g4o``/``hsys_stats_g4o``  the same GRAPE-4 branch on the CPU, over
                        ``oracle/h3_oracle.c`` + ``oracle/g4_oracle.c`` (the
-                       GRAPE-4 ABI on the oracle's pipeline restatement).
+                       GRAPE-4 ABI on the oracle's pipeline restatement);
+* ``kira_g6o``/``hsys_stats_g6o``/``hscale_g6o``/``get_densities_g6o``  the
+                       GRAPE-6 branch on the CPU, over
+                       ``oracle/g6_abi_oracle.c`` + ``oracle/g6_oracle.c``.
 
 Nothing here is shipped; the outputs are git-ignored.  Usage:
 ``python oracle/build_ref.py [--jobs N] [--ref PATH]``.
@@ -165,11 +168,12 @@ def main():
     add(os.path.join(HERE, "ref_force.C"), harness_obj)
     g4_obj = os.path.join(OUT, "obj", "hdyn_grape4_half_chip.o")
     add(os.path.join(src, "node/dyn/hdyn/evolve/hdyn_grape4.C"), g4_obj, extra=["-DUSE_HALF_CHIP=1"])
-    h3o_objs = []
-    for f in ("h3_oracle.c", "g4_oracle.c"):
-        obj = os.path.join(OUT, "obj", "oracle__" + f + ".o")
-        add(os.path.join(HERE, f), obj, extra=["-ffp-contract=off"], c=True)
-        h3o_objs.append(obj)
+    oobj = {}
+    for f in ("h3_oracle.c", "g4_oracle.c", "g6_abi_oracle.c", "g6_oracle.c"):
+        oobj[f] = os.path.join(OUT, "obj", "oracle__" + f + ".o")
+        add(os.path.join(HERE, f), oobj[f], extra=["-ffp-contract=off"], c=True)
+    h3o_objs = [oobj["h3_oracle.c"], oobj["g4_oracle.c"]]
+    g6o_objs = [oobj["g6_abi_oracle.c"], oobj["g6_oracle.c"]]
     sim_src = os.path.join(src, "harpsims", "harp3fastsim.c")
     sim_obj = os.path.join(OUT, "obj", "harp3fastsim.o")
     add(sim_src, sim_obj, extra=["-std=gnu89"], c=True)
@@ -210,6 +214,12 @@ def main():
         exe = os.path.join(OUT, name + "_g4o")
         if not up_to_date(exe, [tool_objs[name], g4_obj, lib, stubs] + h3o_objs):
             run(["g++", "-o", exe, tool_objs[name], g4_obj, lib] + h3o_objs + [stubs] + link_tail)
+
+    # ... and their GRAPE-6 branch over the CPU oracle.
+    for name in ("kira", "hsys_stats", "hscale", "get_densities"):
+        exe = os.path.join(OUT, name + "_g6o")
+        if not up_to_date(exe, [tool_objs[name], lib, stubs] + g6o_objs):
+            run(["g++", "-o", exe, tool_objs[name], lib] + g6o_objs + [stubs] + link_tail)
 
     # kira and hsys_stats driving the GPU engine through the unchanged g6 ABI.
     g6lib_dir = os.path.join(REPO, "starlab_b200", "lib")
