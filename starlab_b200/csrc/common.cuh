@@ -36,7 +36,7 @@ struct __align__(16) JRecMixed {
 // side by side, so one 8-byte half of a float4 is a ready FP32x2 operand.
 struct __align__(16) JPairMixed {
     float4 hxy;   // hx0 hx1 hy0 hy1
-    float4 hzm;   // hz0 hz1 m0 m1
+    float4 hzm;   // hz0 hz1 -m0/8 -m1/8 (the pair kernel's Newton step yields -2/r)
     float4 lxy;   // lx0 lx1 ly0 ly1
     float4 lzi;   // lz0 lz1 index0 index1 (int bits)
     float4 vxy;   // vx0 vx1 vy0 vy1

@@ -219,7 +219,7 @@ __global__ void ens_predict_kernel(EnsDev d) {
     if (d.kmode == kKernMixedP) {
         JPairMixed r;
         r.hxy = make_float4(hi[0][0], hi[1][0], hi[0][1], hi[1][1]);
-        r.hzm = make_float4(hi[0][2], hi[1][2], mm[0], mm[1]);
+        r.hzm = make_float4(hi[0][2], hi[1][2], -0.125f * mm[0], -0.125f * mm[1]);  // -m/8: see JPairMixed
         r.lxy = make_float4(lo[0][0], lo[1][0], lo[0][1], lo[1][1]);
         r.lzi = make_float4(lo[0][2], lo[1][2], __int_as_float(id[0]), __int_as_float(id[1]));
         r.vxy = make_float4(vv[0][0], vv[1][0], vv[0][1], vv[1][1]);

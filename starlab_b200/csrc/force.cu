@@ -272,7 +272,7 @@ __device__ __forceinline__ void interact(StateF64 &s, const double4 &pos, const 
 struct StateMixedP {
     float2 nxh, nyh, nzh, nxl, nyl, nzl, nvx, nvy, nvz;
     float h2;
-    float2 ax, ay, az, jx, jy, jz, pm;  // FP32 sums since the last fold; pm = sum m/r
+    float2 ax, ay, az, jx, jy, jz, pm;  // FP32 sums since the last fold; pm = sum m/(4r)
     double Ax, Ay, Az, Jx, Jy, Jz, Pt;
     float nr2;
     int nj, idx, i;
@@ -332,13 +332,18 @@ __device__ __forceinline__ void interact_pair(StateMixedP &s, const JPairMixed &
         r2nn.y = self1 ? FLT_MAX : r2nn.y;
     }
     float2 y = make_float2(rsqrt_approx(r2.x), rsqrt_approx(r2.y));
-    // One Newton-Raphson step: y <- y (1.5 - 0.5 r2 y^2).
-    const float2 nhy = __fmul2_rn(__fmul2_rn(r2, dup(-0.5f)), y);
-    y = __fmul2_rn(y, __ffma2_rn(nhy, y, dup(1.5f)));
+    // One Newton-Raphson step, kept at -2 times its value:
+    // y' = y (r2 y^2 - 3) = -2 y (1.5 - 0.5 r2 y^2), one instruction fewer
+    // than the textbook form.  Every product below is the scalar kernel's
+    // scaled by a power of two (exact), and the record's mass is -m/8, so
+    // mr3 = (-m/8)(-2y)(4 y^2) and a3 = (-0.75 rv)(4 y^2) come out
+    // bit-identical to the textbook form; pm sums m/(4r).
+    const float2 ry = __fmul2_rn(r2, y);
+    y = __fmul2_rn(y, __ffma2_rn(ry, y, dup(-3.f)));
     const float2 r2inv = __fmul2_rn(y, y);
     const float2 mr = __fmul2_rn(m, y);
     const float2 mr3 = __fmul2_rn(mr, r2inv);
-    const float2 a3 = __fmul2_rn(__fmul2_rn(rv, dup(-3.f)), r2inv);
+    const float2 a3 = __fmul2_rn(__fmul2_rn(rv, dup(-0.75f)), r2inv);
     s.pm = __fadd2_rn(s.pm, mr);
     s.ax = __ffma2_rn(mr3, dx, s.ax);
     s.ay = __ffma2_rn(mr3, dy, s.ay);
@@ -369,7 +374,7 @@ __device__ __forceinline__ void fold(StateMixedP &s) {
     s.Jx += (double)s.jx.x; s.Jx += (double)s.jx.y;
     s.Jy += (double)s.jy.x; s.Jy += (double)s.jy.y;
     s.Jz += (double)s.jz.x; s.Jz += (double)s.jz.y;
-    s.Pt -= (double)s.pm.x; s.Pt -= (double)s.pm.y;
+    s.Pt -= 4.0 * (double)s.pm.x; s.Pt -= 4.0 * (double)s.pm.y;  // pm sums m/(4r)
     s.ax = s.ay = s.az = s.jx = s.jy = s.jz = s.pm = make_float2(0.f, 0.f);
 }
 

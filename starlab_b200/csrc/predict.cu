@@ -105,7 +105,7 @@ __global__ void predict_pair_kernel(const double *__restrict__ jraw, const int *
     if (bad) atomicOr(status, ST_RANGE);
     JPairMixed r;
     r.hxy = make_float4(hi[0][0], hi[1][0], hi[0][1], hi[1][1]);
-    r.hzm = make_float4(hi[0][2], hi[1][2], m[0], m[1]);
+    r.hzm = make_float4(hi[0][2], hi[1][2], -0.125f * m[0], -0.125f * m[1]);  // -m/8: see JPairMixed
     r.lxy = make_float4(lo[0][0], lo[1][0], lo[0][1], lo[1][1]);
     r.lzi = make_float4(lo[0][2], lo[1][2], __int_as_float(id[0]), __int_as_float(id[1]));
     r.vxy = make_float4(v[0][0], v[1][0], v[0][1], v[1][1]);
