@@ -830,10 +830,12 @@ ForceConfig choose_config(int kmode, int ni, int nj_pad, int num_sms, bool nb) {
     c.warps = kMaxWarps;
     c.il = ni >= 32 ? 32 : (ni > 1 ? 8 : 1);
     if (c.il == 8 && ni > 8) c.il = 32;
-    // Register blocking: the scalar mixed layout gains from 2 i per thread;
-    // the paired layout already reuses each loaded j-pair twice and runs out
-    // of registers at 2 (measured: 91 ms vs 95 ms for the N = 262144 sweep).
-    c.r = (kmode == kKernMixedDS && c.il == 32 && ni >= 8192) ? 2 : 1;
+    // Register blocking: the scalar mixed layout gains from 2 i per thread,
+    // and so does FP64 (two independent FP64 chains per thread hide part of
+    // the dependency waits: 10.48 vs 10.58 ms for 16384 x 262144); the
+    // paired layout already reuses each loaded j-pair twice and runs out of
+    // registers at 2 (measured: 91 ms vs 95 ms for the N = 262144 sweep).
+    c.r = ((kmode == kKernMixedDS || kmode == kKernF64) && c.il == 32 && ni >= 8192) ? 2 : 1;
     // i-groups per CTA: as many warps on distinct i as there are i's.
     int groups_needed = (ni + c.il * c.r - 1) / (c.il * c.r);
     int G = 1;
