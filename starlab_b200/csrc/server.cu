@@ -52,6 +52,20 @@ struct Request {
     std::condition_variable cv;  // signalled once, when done (waits on the server mutex)
 };
 
+// Per-batch and per-call timing records, kept when G6B200_SRV_TRACE names a
+// file (written as CSV at shutdown): where the time of a served call goes.
+struct BatchTrace {
+    int lane, nb;
+    long long ni_total, interactions;
+    double t_begin, t_launch, t_end, gpu_ms;
+    int grew;
+};
+struct CallTrace {
+    long long id;
+    int lane, cluster, ni, nj;
+    double t_submit, t_batch, t_done;
+};
+
 struct ServerStats {
     long long batches = 0, requests = 0, interactions = 0, max_batch = 0;
     double gpu_ms = 0;      // device time of the batches (events)
@@ -82,6 +96,7 @@ struct Lane {
     ForceParams *h_items = nullptr, *d_items = nullptr;
     int *h_pre = nullptr, *d_pre = nullptr;
     int *d_counter = nullptr;
+    std::vector<void *> retired_host;  // pinned buffers replaced by larger ones (freed at shutdown)
 };
 
 class Server {
@@ -136,6 +151,11 @@ class Server {
     bool stop_ = false;
     bool started_ = false;
     ServerStats stats_;
+    std::string trace_path_;
+    double t_created_ = now();
+    std::vector<BatchTrace> batch_trace_;
+    std::vector<CallTrace> call_trace_;
+    void write_trace();
     Lane lanes_[2];
     int ctas_ = 0;
     ForceConfig cfg_{};
@@ -147,6 +167,7 @@ int Server::start() {
         return -1;
     }
     if (const char *e = getenv("G6B200_SRV_SMALL")) small_max_ = atoll(e);
+    if (const char *e = getenv("G6B200_SRV_TRACE")) trace_path_ = e;
     kmode_ = precision_ == kModeF64 ? kKernF64 : kKernMixedP;
     int lo = 0, hi = 0;
     cudaDeviceGetStreamPriorityRange(&lo, &hi);  // hi = greatest priority (numerically lowest)
@@ -166,19 +187,32 @@ int Server::start() {
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device_);
     ctas_ = batch_ctas(kmode_, cfg_, sms);
+    // Pre-size the lanes (i-records, split partials, per-call predicted
+    // j-sets, work items) for batches of tens of clusters of up to 2^17
+    // particles: about 0.4 GB of HBM and 50 MB of pinned host memory.
+    const size_t rec = kmode_ == kKernF64 ? sizeof(JRecF64) : sizeof(JRecMixed);
+    if (ensure(lanes_[0], 1 << 17, 1 << 19, rec << 21, 1024) || ensure(lanes_[1], 1 << 18, 1 << 19, rec << 22, 256) ||
+        cudaStreamSynchronize(lanes_[0].stream) != cudaSuccess || cudaStreamSynchronize(lanes_[1].stream) != cudaSuccess) {
+        err = "server: lane buffers";
+        return -1;
+    }
     for (int k = 0; k < 2; ++k) lanes_[k].thread = std::thread([this, k] { loop(lanes_[k]); });
     started_ = true;
     return 0;
 }
 
 void Server::free_lane(Lane &L) {
+    if (L.stream) cudaStreamSynchronize(L.stream);
+    for (void *p : L.retired_host) cudaFreeHost(p);
     if (L.h_irec) cudaFreeHost(L.h_irec);
     if (L.h_out) cudaFreeHost(L.h_out);
     if (L.h_items) cudaFreeHost(L.h_items);
     if (L.h_pre) cudaFreeHost(L.h_pre);
     for (void *p : {(void *)L.d_irec, (void *)L.d_out, (void *)L.d_part, (void *)L.d_items, (void *)L.d_pre,
-                    (void *)L.d_counter, (void *)L.d_jrec})
-        if (p) cudaFree(p);
+                    (void *)L.d_jrec})
+        if (p) cudaFreeAsync(p, L.stream);
+    if (L.d_counter) cudaFree(L.d_counter);
+    if (L.stream) cudaStreamSynchronize(L.stream);
     for (cudaEvent_t e : L.ready) cudaEventDestroy(e);
     L.ready.clear();
     for (cudaEvent_t e : {L.ev_clear, L.ev_t0, L.ev_t1})
@@ -197,6 +231,7 @@ void Server::shutdown() {
     cv_mem_.notify_all();
     for (Lane &L : lanes_)
         if (L.thread.joinable()) L.thread.join();
+    write_trace();
     cudaSetDevice(device_);
     for (auto &kv : clusters_) kv.second->eng.reset();
     clusters_.clear();
@@ -338,6 +373,9 @@ void Server::loop(Lane &L) {
                 if (rc) r->rc = rc;
                 r->done = true;
                 r->t_done = t;
+                if (!trace_path_.empty())
+                    call_trace_.push_back({r->id, L.id, r->cluster, r->ni, r->nj, r->t_submit - t_created_,
+                                           tb0 - t_created_, t - t_created_});
                 stats_.queue_ms += (tb0 - r->t_submit) * 1e3;
                 auto it = clusters_.find(r->cluster);
                 if (it != clusters_.end()) it->second->inflight--;
@@ -349,38 +387,43 @@ void Server::loop(Lane &L) {
     }
 }
 
+// Lane buffers grow geometrically.  Growth never synchronises the device
+// (the other lane keeps running): device buffers are stream-ordered
+// allocations on the lane's own stream, and replaced pinned buffers are kept
+// until shutdown instead of being freed (cudaFreeHost may synchronise).
+// start() pre-sizes both lanes so that growth is rare in service.
 int Server::ensure(Lane &L, size_t ni_total, size_t parts, size_t jrec_bytes, int n_items) {
+    auto dev_realloc = [&](auto *&ptr, size_t bytes) {
+        if (ptr) cudaFreeAsync(ptr, L.stream);
+        ptr = nullptr;
+        return cudaMallocAsync(reinterpret_cast<void **>(&ptr), bytes, L.stream) == cudaSuccess;
+    };
+    auto host_realloc = [&](auto *&ptr, size_t bytes) {
+        if (ptr) L.retired_host.push_back(ptr);
+        ptr = nullptr;
+        return cudaMallocHost(reinterpret_cast<void **>(&ptr), bytes) == cudaSuccess;
+    };
     if (ni_total > L.cap_i) {
         size_t n = std::max(ni_total, L.cap_i * 2);
-        if (L.h_irec) cudaFreeHost(L.h_irec);
-        if (L.d_irec) cudaFree(L.d_irec);
-        if (L.h_out) cudaFreeHost(L.h_out);
-        if (L.d_out) cudaFree(L.d_out);
-        if (cudaMallocHost(&L.h_irec, sizeof(IRec) * n) || cudaMalloc(&L.d_irec, sizeof(IRec) * n) ||
-            cudaMallocHost(&L.h_out, 16 + 60 * n) || cudaMalloc(&L.d_out, 16 + 60 * n))
+        if (!host_realloc(L.h_irec, sizeof(IRec) * n) || !dev_realloc(L.d_irec, sizeof(IRec) * n) ||
+            !host_realloc(L.h_out, 16 + 60 * n) || !dev_realloc(L.d_out, 16 + 60 * n))
             return -1;
         L.cap_i = n;
     }
     if (parts > L.cap_part) {
         size_t n = std::max(parts, L.cap_part * 2);
-        if (L.d_part) cudaFree(L.d_part);
-        if (cudaMalloc(&L.d_part, sizeof(Partial) * n)) return -1;
+        if (!dev_realloc(L.d_part, sizeof(Partial) * n)) return -1;
         L.cap_part = n;
     }
     if (jrec_bytes > L.cap_jrec) {
         size_t n = std::max(jrec_bytes, L.cap_jrec * 2);
-        if (L.d_jrec) cudaFree(L.d_jrec);
-        if (cudaMalloc(&L.d_jrec, n)) return -1;
+        if (!dev_realloc(L.d_jrec, n)) return -1;
         L.cap_jrec = n;
     }
     if (n_items > L.cap_items) {
         int n = std::max(n_items, L.cap_items * 2);
-        if (L.h_items) cudaFreeHost(L.h_items);
-        if (L.d_items) cudaFree(L.d_items);
-        if (L.h_pre) cudaFreeHost(L.h_pre);
-        if (L.d_pre) cudaFree(L.d_pre);
-        if (cudaMallocHost(&L.h_items, sizeof(ForceParams) * n) || cudaMalloc(&L.d_items, sizeof(ForceParams) * n) ||
-            cudaMallocHost(&L.h_pre, sizeof(int) * 2 * (n + 1)) || cudaMalloc(&L.d_pre, sizeof(int) * 2 * (n + 1)))
+        if (!host_realloc(L.h_items, sizeof(ForceParams) * n) || !dev_realloc(L.d_items, sizeof(ForceParams) * n) ||
+            !host_realloc(L.h_pre, sizeof(int) * 2 * (n + 1)) || !dev_realloc(L.d_pre, sizeof(int) * 2 * (n + 1)))
             return -1;
         L.cap_items = n;
     }
@@ -395,6 +438,8 @@ int Server::ensure(Lane &L, size_t ni_total, size_t parts, size_t jrec_bytes, in
 int Server::run_batch(Lane &L, std::vector<std::shared_ptr<Request>> &batch) {
     const int nb = (int)batch.size();
     if (nb == 0) return 0;
+    const double t_begin = now();
+    const size_t caps_before = L.cap_i + L.cap_part + L.cap_jrec + (size_t)L.cap_items;
     const int T = tile_of(kmode_);
     const size_t rec = kmode_ == kKernF64 ? sizeof(JRecF64) : sizeof(JRecMixed);
     size_t ni_total = 0, parts = 0, jbytes = 0;
@@ -466,6 +511,7 @@ int Server::run_batch(Lane &L, std::vector<std::shared_ptr<Request>> &batch) {
     }
     L.h_pre[nb] = task;
     L.h_pre[2 * nb + 1] = (int)ioff;
+    const double t_launch = now();
     cudaEventRecord(L.ev_t0, L.stream);
     cudaMemcpyAsync(L.d_irec, L.h_irec, sizeof(IRec) * ni_total, cudaMemcpyHostToDevice, L.stream);
     cudaMemcpyAsync(L.d_items, L.h_items, sizeof(ForceParams) * nb, cudaMemcpyHostToDevice, L.stream);
@@ -538,8 +584,27 @@ int Server::run_batch(Lane &L, std::vector<std::shared_ptr<Request>> &batch) {
         stats_.interactions += inter;
         stats_.max_batch = std::max<long long>(stats_.max_batch, nb);
         stats_.gpu_ms += ms;
+        if (!trace_path_.empty()) {
+            const size_t caps_after = L.cap_i + L.cap_part + L.cap_jrec + (size_t)L.cap_items;
+            batch_trace_.push_back({L.id, nb, (long long)ni_total, inter, t_begin - t_created_,
+                                    t_launch - t_created_, now() - t_created_, ms, caps_after != caps_before});
+        }
     }
     return 0;
+}
+
+void Server::write_trace() {
+    if (trace_path_.empty()) return;
+    FILE *f = fopen(trace_path_.c_str(), "w");
+    if (!f) return;
+    fprintf(f, "kind,lane,n,ni,interactions_or_nj,t0,t1,t2,gpu_ms_or_cluster,grew_or_id\n");
+    for (const BatchTrace &b : batch_trace_)
+        fprintf(f, "batch,%d,%d,%lld,%lld,%.6f,%.6f,%.6f,%.4f,%d\n", b.lane, b.nb, b.ni_total, b.interactions,
+                b.t_begin, b.t_launch, b.t_end, b.gpu_ms, b.grew);
+    for (const CallTrace &c : call_trace_)
+        fprintf(f, "call,%d,1,%d,%d,%.6f,%.6f,%.6f,%d,%lld\n", c.lane, c.ni, c.nj, c.t_submit, c.t_batch, c.t_done,
+                c.cluster, c.id);
+    fclose(f);
 }
 
 }  // namespace g6
