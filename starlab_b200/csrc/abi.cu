@@ -225,13 +225,10 @@ int g6b200_set_j_particles(int cluster_id, int n, const int *address, const int 
                            const double (*a2)[3], const double (*v)[3], const double (*x)[3]) {
     g6::Engine *e = engine(cluster_id);
     if (!e) return -1;
-    for (int k = 0; k < n; ++k) {
-        int a = address ? address[k] : k;
-        int id = index ? index[k] : a;
-        if (e->set_j(a, id, tj[k], mass[k], k18 ? k18[k] : nullptr, j6[k], a2[k], v[k], x[k])) {
-            note(e);
-            return -1;
-        }
+    if (e->set_j_bulk(n, address, index, tj, mass, k18 ? &k18[0][0] : nullptr, &j6[0][0], &a2[0][0], &v[0][0],
+                      &x[0][0])) {
+        note(e);
+        return -1;
     }
     return 0;
 }

@@ -123,7 +123,7 @@ void Engine::close() {
     dfree(d_jraw_); dfree(d_jindex_); dfree(d_jrec_);
     dfree(d_stage_vals_); dfree(d_stage_addr_); dfree(d_stage_index_);
     dfree(d_irec_); dfree(d_out_); dfree(d_part_); dfree(d_tile_cnt_);
-    dfree(d_nb_count_); dfree(d_nb_list_); dfree(d_nb_sorted_); dfree(d_nb_off_);
+    dfree(d_nb_count_); dfree(d_nb_list_); dfree(d_nb_sorted_); dfree(d_nb_off_); dfree(d_bulk_);
     hfree(h_stage_vals_); hfree(h_stage_addr_); hfree(h_stage_index_);
     hfree(h_irec_); hfree(h_out_); hfree(h_nb_off_); hfree(h_nb_count_);
     hfree(h_ieps2_); dfree(d_ieps2_);
@@ -134,6 +134,7 @@ void Engine::close() {
     d_stage_vals_ = nullptr; d_stage_addr_ = nullptr; d_stage_index_ = nullptr;
     d_irec_ = nullptr; d_out_ = nullptr; d_part_ = nullptr; d_tile_cnt_ = nullptr;
     d_nb_count_ = nullptr; d_nb_list_ = nullptr; d_nb_sorted_ = nullptr; d_nb_off_ = nullptr;
+    d_bulk_ = nullptr; bulk_cap_ = 0; bulk_mark_.clear();
     h_stage_vals_ = nullptr; h_stage_addr_ = nullptr; h_stage_index_ = nullptr;
     h_irec_ = nullptr; h_out_ = nullptr; h_nb_off_ = nullptr; h_nb_count_ = nullptr;
     h_ieps2_ = nullptr; d_ieps2_ = nullptr;
@@ -272,6 +273,94 @@ int Engine::flush_j() {
     stats_.h2d_bytes += (long long)n * (JF_COUNT * 8 + 8);
     for (int k = 0; k < n; ++k) slot_of_[h_stage_addr_[k]] = -1;
     n_staged_ = 0;
+    pred_valid_ = false;
+    return 0;
+}
+
+int Engine::set_j_bulk(int n, const int *address, const int *index, const double *tj, const double *mass,
+                       const double *k18, const double *j6, const double *a2, const double *v, const double *x) {
+    auto one_by_one = [&]() {
+        for (int k = 0; k < n; ++k) {
+            const int a = address ? address[k] : k;
+            if (set_j(a, index ? index[k] : a, tj[k], mass[k], k18 ? k18 + 3 * (size_t)k : nullptr,
+                      j6 + 3 * (size_t)k, a2 + 3 * (size_t)k, v + 3 * (size_t)k, x + 3 * (size_t)k))
+                return -1;
+        }
+        return 0;
+    };
+    constexpr int kBulkMin = 4096;
+    if (n <= 0) return 0;
+    if (n < kBulkMin) return one_by_one();
+    if (!open_ && open(env_int("G6B200_DEVICE", 0), 0)) return -1;
+    int amax = n - 1;
+    if (address) {
+        amax = -1;
+        for (int k = 0; k < n; ++k) {
+            if (address[k] < 0) {
+                last_error = "g6b200: negative j address";
+                return -1;
+            }
+            amax = std::max(amax, address[k]);
+        }
+        if ((size_t)amax + 1 > bulk_mark_.size()) bulk_mark_.resize((size_t)amax + 1, 0);
+        if (++bulk_gen_ == 0) {
+            std::fill(bulk_mark_.begin(), bulk_mark_.end(), 0u);
+            bulk_gen_ = 1;
+        }
+        for (int k = 0; k < n; ++k) {
+            if (bulk_mark_[address[k]] == bulk_gen_) return one_by_one();  // repeated address: last write wins
+            bulk_mark_[address[k]] = bulk_gen_;
+        }
+    }
+    if (ensure_capacity(amax)) return -1;
+    if (flush_j()) return -1;  // earlier single updates land first
+    G6_CHECK(cudaSetDevice(device_), "cudaSetDevice");
+    const size_t nd = (size_t)n, vec = 24 * nd;
+    const size_t bytes = 16 * nd + 5 * vec + 8 * nd + 64;
+    if (bytes > bulk_cap_) {
+        G6_CHECK(cudaStreamSynchronize(stream_), "sync");
+        if (d_bulk_) cudaFree(d_bulk_);
+        d_bulk_ = nullptr;
+        bulk_cap_ = 0;
+        G6_CHECK(cudaMalloc(&d_bulk_, bytes), "bulk j");
+        bulk_cap_ = bytes;
+    }
+    unsigned char *p = d_bulk_;
+    auto put = [&](const void *src, size_t b) -> const void * {
+        if (!src) return nullptr;
+        unsigned char *dst = p;
+        p += (b + 15) / 16 * 16;
+        return cudaMemcpyAsync(dst, src, b, cudaMemcpyHostToDevice, stream_) == cudaSuccess ? dst : nullptr;
+    };
+    BulkJ b;
+    b.t = static_cast<const double *>(put(tj, 8 * nd));
+    b.m = static_cast<const double *>(put(mass, 8 * nd));
+    b.x = static_cast<const double *>(put(x, vec));
+    b.v = static_cast<const double *>(put(v, vec));
+    b.a2 = static_cast<const double *>(put(a2, vec));
+    b.j6 = static_cast<const double *>(put(j6, vec));
+    b.k18 = static_cast<const double *>(put(k18, vec));
+    b.addr = static_cast<const int *>(put(address, 4 * nd));
+    b.index = static_cast<const int *>(put(index, 4 * nd));
+    if (!b.t || !b.m || !b.x || !b.v || !b.a2 || !b.j6 || (k18 && !b.k18) || (address && !b.addr) ||
+        (index && !b.index))
+        return fail("bulk j copy", cudaGetLastError());
+    launch_scatter_bulk(stream_, n, b, d_jraw_, d_jindex_, cap_);
+    G6_CHECK(cudaGetLastError(), "bulk scatter launch");
+    stats_.launches++;
+    stats_.h2d_bytes += (long long)(p - d_bulk_);
+    stats_.j_updates += n;
+    double xm = xmax_;
+    for (size_t k = 0; k < 3 * nd; ++k) xm = std::max(xm, std::fabs(x[k]));
+    xmax_ = xm;
+    for (int k = 0; k < n; ++k) {
+        const int a = address ? address[k] : k;
+        const bool ni = index && index[k] != a;
+        if (ni != (bool)nonident_[a]) {
+            nonident_[a] = ni;
+            n_nonident_ += ni ? 1 : -1;
+        }
+    }
     pred_valid_ = false;
     return 0;
 }

@@ -44,6 +44,12 @@ class Engine {
     int set_j(int address, int index, double tj, double mass, const double *k18,
               const double *j6, const double *a2, const double *v, const double *x);
     int flush_j();
+    // Many j-particles at once (tj, mass [n]; k18, j6, a2, v, x [n][3] flat;
+    // address/index/k18 may be null).  Same result as n set_j calls in
+    // order: large uploads with distinct addresses go straight from the
+    // caller's arrays to the device and one scatter kernel.
+    int set_j_bulk(int n, const int *address, const int *index, const double *tj, const double *mass,
+                   const double *k18, const double *j6, const double *a2, const double *v, const double *x);
 
     int firsthalf(int nj, int ni, const int *index, const double (*xi)[3],
                   const double (*vi)[3], double eps2, const double *h2);
@@ -146,6 +152,10 @@ class Engine {
     int *d_stage_addr_ = nullptr, *d_stage_index_ = nullptr;
     std::vector<int> slot_of_;
     cudaEvent_t ev_stage_ = nullptr;
+    unsigned char *d_bulk_ = nullptr;  // device copies of a bulk upload's arrays
+    size_t bulk_cap_ = 0;
+    std::vector<unsigned> bulk_mark_;  // duplicate-address check (generation stamps)
+    unsigned bulk_gen_ = 0;
     bool stage_busy_ = false;
 
     // per-call buffers

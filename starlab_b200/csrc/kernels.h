@@ -89,6 +89,13 @@ struct ForceConfig {
 
 void launch_scatter(cudaStream_t s, int n, const int *addr, const int *index, const double *vals,
                     double *jraw, int *jindex, int cap);
+// Device copies of a caller's j arrays for a bulk upload (addr/index/k18 may
+// be null: addresses 0..n-1, index = address, k18 = 0).
+struct BulkJ {
+    const double *t, *m, *x, *v, *a2, *j6, *k18;
+    const int *addr, *index;
+};
+void launch_scatter_bulk(cudaStream_t s, int n, const BulkJ &b, double *jraw, int *jindex, int cap);
 void launch_predict(cudaStream_t s, int kmode, const double *jraw, const int *jindex, int cap,
                     int nj, int nj_pad, double ti, const FixedScale &fs, void *jrec,
                     unsigned *status);

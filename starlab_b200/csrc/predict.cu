@@ -29,6 +29,30 @@ __global__ void scatter_j_kernel(int n, const int *__restrict__ addr,
     }
 }
 
+// Bulk upload: the caller's arrays, copied as they are (t[n], m[n], x, v,
+// a2, j6, k18 as [n][3]), scattered into the raw j-state.  One thread per
+// (field, particle), so a warp writes one SoA row contiguously when the
+// addresses are.
+__global__ void scatter_bulk_kernel(int n, BulkJ b, double *__restrict__ jraw, int *__restrict__ jindex, int cap) {
+    const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (t >= (long long)n * JF_COUNT) return;
+    const int f = (int)(t / n);
+    const int r = (int)(t - (long long)f * n);
+    const int a = b.addr ? b.addr[r] : r;
+    double val;
+    if (f == JF_T) {
+        val = b.t[r];
+    } else if (f == JF_M) {
+        val = b.m[r];
+    } else {
+        const int g = (f - JF_X) / 3, c = (f - JF_X) % 3;  // x, v, a2, j6, k18 rows follow each other
+        const double *src = g == 0 ? b.x : g == 1 ? b.v : g == 2 ? b.a2 : g == 3 ? b.j6 : b.k18;
+        val = src ? src[3 * (size_t)r + c] : 0.0;
+    }
+    jraw[(size_t)f * cap + a] = val;
+    if (f == JF_T) jindex[a] = b.index ? b.index[r] : a;
+}
+
 __device__ __forceinline__ void predict_one(const double *__restrict__ jraw, int cap, int j,
                                             double ti, double xp[3], double vp[3], double &m) {
     double dt = ti - jraw[(size_t)JF_T * cap + j];
@@ -165,6 +189,13 @@ void launch_scatter(cudaStream_t s, int n, const int *addr, const int *index, co
     int threads = 256;
     unsigned blocks = (unsigned)((total + threads - 1) / threads);
     scatter_j_kernel<<<blocks, threads, 0, s>>>(n, addr, index, vals, jraw, jindex, cap);
+}
+
+void launch_scatter_bulk(cudaStream_t s, int n, const BulkJ &b, double *jraw, int *jindex, int cap) {
+    if (n <= 0) return;
+    const long long total = (long long)n * JF_COUNT;
+    const int threads = 256;
+    scatter_bulk_kernel<<<(unsigned)((total + threads - 1) / threads), threads, 0, s>>>(n, b, jraw, jindex, cap);
 }
 
 void launch_predict(cudaStream_t s, int kmode, const double *jraw, const int *jindex, int cap,

@@ -295,12 +295,9 @@ int Server::set_j(int c, int n, const int *address, const double *tj, const doub
         cl = it->second.get();
     }
     std::lock_guard<std::mutex> lk(cl->mu);
-    for (int k = 0; k < n; ++k) {
-        const int a = address ? address[k] : k;
-        if (cl->eng->set_j(a, a, tj[k], mass[k], nullptr, j6[k], a2[k], v[k], x[k])) {
-            err = cl->eng->last_error;
-            return -1;
-        }
+    if (cl->eng->set_j_bulk(n, address, address, tj, mass, nullptr, &j6[0][0], &a2[0][0], &v[0][0], &x[0][0])) {
+        err = cl->eng->last_error;
+        return -1;
     }
     return 0;
 }

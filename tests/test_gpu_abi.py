@@ -114,6 +114,46 @@ def test_single_particle_upload_equals_batched(oracle):
     e2.close()
 
 
+def test_bulk_upload_equals_single_updates(oracle):
+    """g6b200_set_j_particles of >= 4096 particles takes the bulk path
+    (the caller's arrays copied straight to the device, one scatter kernel):
+    permuted addresses, index != address, a repeated address (last write
+    wins, as n single g6_set_j_particle_ calls), and single updates before
+    and after, must leave exactly the j-memory the single calls leave."""
+    n = 6000
+    m, x, v, a, j = snapshot(n, 21)
+    rng = np.random.default_rng(4)
+    perm = rng.permutation(n).astype(np.int32)
+    index = perm.copy()
+    index[::7] += 100000          # some ids differ from their address
+    dup_addr = perm.copy()
+    dup_addr[-1] = dup_addr[0]    # a repeated address: the later entry wins
+    z = np.zeros(3)
+    e1, e2 = eng(), eng()
+    # a single update staged before the bulk upload, overwritten by it
+    e1.set_j_particle(int(perm[5]), 0.0, 9.0, z, z, z, z, np.ones(3))
+    e1.set_j_particles(0.0, m, j / 6.0, 0.5 * a, v, x, address=perm, index=index)
+    e1.set_j_particles(0.0, m[:10], (j / 6.0)[:10], (0.5 * a)[:10], v[:10], x[:10] * 1.01, address=perm[:10])
+    e1.set_j_particles(0.0, m, j / 6.0, 0.5 * a, v, x, address=dup_addr, index=index)
+    e1.set_j_particle(int(perm[7]), 0.0, m[7], z, (j / 6.0)[7], (0.5 * a)[7], v[7], x[7] * 0.99)
+    for k in range(n):
+        e2.set_j_particle(int(perm[k]), 0.0, m[k], z, (j / 6.0)[k], (0.5 * a)[k], v[k], x[k], index=int(index[k]))
+    e2.set_j_particle(int(dup_addr[-1]), 0.0, m[-1], z, (j / 6.0)[-1], (0.5 * a)[-1], v[-1], x[-1],
+                      index=int(index[-1]))
+    e2.set_j_particle(int(perm[7]), 0.0, m[7], z, (j / 6.0)[7], (0.5 * a)[7], v[7], x[7] * 0.99)
+    ti = 1.0 / 512
+    idx = index[:400]
+    xi, vi = x[:400] + 1e-3, v[:400]
+    for e in (e1, e2):
+        e.set_ti(ti)
+    r1 = e1.force(n, idx, xi, vi, 1e-6)
+    r2 = e2.force(n, idx, xi, vi, 1e-6)
+    for p, q in zip(r1, r2):
+        assert np.array_equal(p, q)
+    e1.close()
+    e2.close()
+
+
 def test_open_close_reset_cycles(oracle):
     from starlab_b200 import load_library
     lib = load_library()
