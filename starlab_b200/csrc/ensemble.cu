@@ -78,41 +78,42 @@ __device__ __forceinline__ void predict_state(const EnsDev &d, int g, double tb,
 // mode 0: next block; mode 1: every particle at its current time (start of
 // the run, or an energy evaluation when all times are equal).
 __global__ void __launch_bounds__(256) ens_schedule_kernel(EnsDev d, int mode) {
-    __shared__ double s_min[256];
-    __shared__ int s_cnt[256];
-    const int c = blockIdx.x, tid = threadIdx.x;
-    const int n = d.n[c], o = d.off[c], pad_end = d.off[c + 1];
+    __shared__ double s_wmin[8];
+    __shared__ int s_wcnt[8];
+    const int c = blockIdx.x, tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+    const int n = d.n[c], o = d.off[c], span = d.off[c + 1] - o;  // span: n padded to 256
     double tmin = DBL_MAX;
     if (mode == 0)
         for (int i = tid; i < n; i += 256) tmin = fmin(tmin, d.t[o + i] + d.dt[o + i]);
-    s_min[tid] = tmin;
+#pragma unroll
+    for (int k = 16; k > 0; k >>= 1) tmin = fmin(tmin, __shfl_xor_sync(0xffffffffu, tmin, k));
+    if (lane == 0) s_wmin[w] = tmin;
     __syncthreads();
-    for (int w = 128; w > 0; w >>= 1) {
-        if (tid < w) s_min[tid] = fmin(s_min[tid], s_min[tid + w]);
-        __syncthreads();
-    }
-    const double tb = mode == 0 ? s_min[0] : (n > 0 ? d.t[o] : 0.0);
+    for (int k = 0; k < 8; ++k) tmin = fmin(tmin, s_wmin[k]);
+    const double tb = mode == 0 ? tmin : (n > 0 ? d.t[o] : 0.0);
     const bool active = n > 0 && (mode != 0 || tb <= d.t_end);
-    const int chunk = (n + 255) / 256;
-    const int b = tid * chunk, e = min(b + chunk, n);
-    int local = 0;
-    for (int i = b; i < e; ++i) local += active && (mode != 0 || d.t[o + i] + d.dt[o + i] == tb);
-    s_cnt[tid] = local;
-    __syncthreads();
-    for (int w = 1; w < 256; w <<= 1) {
-        const int add = tid >= w ? s_cnt[tid - w] : 0;
+    // Ordered compaction of the block members, 256 particles per step
+    // (coalesced): slot = members before this particle in address order.
+    int running = 0;
+    for (int base = 0; base < span; base += 256) {
+        const int i = base + tid;
+        const bool mem = i < n && active && (mode != 0 || d.t[o + i] + d.dt[o + i] == tb);
+        const unsigned bal = __ballot_sync(0xffffffffu, mem);
+        if (lane == 0) s_wcnt[w] = __popc(bal);
         __syncthreads();
-        s_cnt[tid] += add;
+        int woff = 0, tot = 0;
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            const int v = s_wcnt[k];
+            woff += k < w ? v : 0;
+            tot += v;
+        }
+        d.slot[o + i] = mem ? running + woff + __popc(bal & ((1u << lane) - 1u)) : -1;
+        running += tot;
         __syncthreads();
     }
-    int k = s_cnt[tid] - local;
-    for (int i = b; i < e; ++i) {
-        const bool mem = active && (mode != 0 || d.t[o + i] + d.dt[o + i] == tb);
-        d.slot[o + i] = mem ? k++ : -1;
-    }
-    for (int i = n + tid; i < pad_end - o; i += 256) d.slot[o + i] = -1;
     if (tid == 0) {
-        const int total = s_cnt[255];
+        const int total = running;
         d.count[c] = total;
         d.tblock[c] = tb;
         ForceParams p{};
@@ -137,23 +138,75 @@ __global__ void __launch_bounds__(256) ens_schedule_kernel(EnsDev d, int mode) {
     }
 }
 
-__global__ void ens_scan_kernel(EnsDev d) {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
-    int t = 0, ii = 0, act = 0;
-    unsigned long long inter = 0;
-    for (int c = 0; c < d.nc; ++c) {
-        d.task0[c] = t;
-        d.ipre[c] = ii;
-        t += d.ntask[c];
-        ii += d.count[c];
-        act += d.count[c] > 0;
-        inter += (unsigned long long)d.count[c] * (unsigned long long)d.n[c];
+// Exclusive prefix sums of the clusters' task and member counts, the count
+// of active clusters and the interaction total: one CTA of 1024 threads,
+// each owning a contiguous run of clusters; warp-shuffle scans.
+__global__ void __launch_bounds__(1024) ens_scan_kernel(EnsDev d) {
+    __shared__ int s_t[32], s_i[32], s_a[32];
+    __shared__ unsigned long long s_x[32];
+    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+    const int per = (d.nc + 1023) / 1024;
+    const int b = min(tid * per, d.nc), e = min(b + per, d.nc);
+    int lt = 0, li = 0, la = 0;
+    unsigned long long lx = 0;
+    for (int c = b; c < e; ++c) {
+        const int cnt = d.count[c];
+        lt += d.ntask[c];
+        li += cnt;
+        la += cnt > 0;
+        lx += (unsigned long long)cnt * (unsigned long long)d.n[c];
     }
-    d.task0[d.nc] = t;
-    d.ipre[d.nc] = ii;
-    *d.active = act;
-    *d.interactions += inter;
-    *d.counter = 0;
+    // inclusive warp scans of lt, li; warp sums of la, lx
+    int it = lt, ii = li;
+#pragma unroll
+    for (int k = 1; k < 32; k <<= 1) {
+        const int a1 = __shfl_up_sync(0xffffffffu, it, k), a2 = __shfl_up_sync(0xffffffffu, ii, k);
+        if (lane >= k) {
+            it += a1;
+            ii += a2;
+        }
+    }
+    int sa = la;
+    unsigned long long sx = lx;
+#pragma unroll
+    for (int k = 16; k > 0; k >>= 1) {
+        sa += __shfl_xor_sync(0xffffffffu, sa, k);
+        sx += __shfl_xor_sync(0xffffffffu, sx, k);
+    }
+    if (lane == 31) {
+        s_t[w] = it;
+        s_i[w] = ii;
+    }
+    if (lane == 0) {
+        s_a[w] = sa;
+        s_x[w] = sx;
+    }
+    __syncthreads();
+    int wt = 0, wi = 0;
+    for (int k = 0; k < w; ++k) {
+        wt += s_t[k];
+        wi += s_i[k];
+    }
+    int t = wt + it - lt, i2 = wi + ii - li;  // exclusive prefix of this thread's run
+    for (int c = b; c < e; ++c) {
+        d.task0[c] = t;
+        d.ipre[c] = i2;
+        t += d.ntask[c];
+        i2 += d.count[c];
+    }
+    if (tid == 1023) {
+        int act = 0;
+        unsigned long long inter = 0;
+        for (int k = 0; k < 32; ++k) {
+            act += s_a[k];
+            inter += s_x[k];
+        }
+        d.task0[d.nc] = t;
+        d.ipre[d.nc] = i2;
+        *d.active = act;
+        *d.interactions += inter;
+        *d.counter = 0;
+    }
 }
 
 // Paired mixed records (one thread per pair) or FP64 records (one thread
@@ -241,13 +294,7 @@ __host__ __device__ inline double pow2_floor(double x) {
 // Hermite corrector (FP64) and the next block step.  mode 1 = start: take
 // the forces as the initial acc/jerk and choose the first step from
 // eta_s |a| / |j|.
-__global__ void ens_correct_kernel(EnsDev d, int mode) {
-    const int g = blockIdx.x * blockDim.x + threadIdx.x;
-    if (g >= d.ntot) return;
-    const int s = d.slot[g];
-    if (s < 0) return;
-    const int c = d.cid[g];
-    const int o = d.off[c];
+__device__ __forceinline__ void correct_one(const EnsDev &d, int mode, int c, int o, int s, int g) {
     const double tb = d.tblock[c];
     const size_t k = (size_t)o + s;
     double a1[3], j1[3];
@@ -298,6 +345,21 @@ __global__ void ens_correct_kernel(EnsDev d, int mode) {
     while (dtn > kDtMin && (fmod(tb, dtn) != 0.0 || (tb < d.t_end && tb + dtn > d.t_end))) dtn *= 0.5;
     d.t[g] = tb;
     d.dt[g] = fmax(dtn, kDtMin);
+}
+
+// Grid-stride over the block members only (ipre[nc] of them): member m is
+// slot s of cluster c, particle o + irec[o + s].index.
+__global__ void ens_correct_kernel(EnsDev d, int mode) {
+    const int total = d.ipre[d.nc];
+    for (int m = blockIdx.x * blockDim.x + threadIdx.x; m < total; m += gridDim.x * blockDim.x) {
+        int lo = 0, hi = d.nc - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (d.ipre[mid] <= m) lo = mid; else hi = mid - 1;
+        }
+        const int c = lo, s = m - d.ipre[c], o = d.off[c];
+        correct_one(d, mode, c, o, s, o + d.irec[o + s].index);
+    }
 }
 
 // Before a run: no step may jump over t_end, so every particle lands on it
@@ -538,7 +600,7 @@ int Ensemble::push_host_state() {
 
 int Ensemble::iteration(int mode) {
     ens_schedule_kernel<<<nc_, 256, 0, stream_>>>(d_, mode);
-    ens_scan_kernel<<<1, 32, 0, stream_>>>(d_);
+    ens_scan_kernel<<<1, 1024, 0, stream_>>>(d_);
     const int per = kmode_ == kKernMixedP ? 2 : 1;
     const int units = (ntot_ / per + 255) / 256;
     ens_predict_kernel<<<units, 256, 0, stream_>>>(d_);
@@ -552,7 +614,7 @@ int Ensemble::iteration(int mode) {
     ba.one_task_per_cta = 0;
     cudaError_t e = launch_force_batch(stream_, kmode_, d_.cfg, ba, ctas_, ntot_, false, true);
     if (e != cudaSuccess) return fail("force launch", e);
-    if (mode != 2) ens_correct_kernel<<<(ntot_ + 255) / 256, 256, 0, stream_>>>(d_, mode);
+    if (mode != 2) ens_correct_kernel<<<4 * num_sms_, 256, 0, stream_>>>(d_, mode);
     return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }
 

@@ -750,21 +750,23 @@ __global__ void __launch_bounds__(256, MinBlocks<K, R>::value) batch_force_kerne
 }
 
 // Split reduction for every i of every item with nsplit > 1; ipre[k] is the
-// prefix sum of the items' ni.
+// prefix sum of the items' ni (read on the device, so a launch captured in a
+// graph serves batches of any size: grid-stride over ipre[n_items]).
 __global__ void batch_reduce_kernel(const BatchArgs a) {
-    const int gi = blockIdx.x * blockDim.x + threadIdx.x;
-    if (gi >= a.ipre[a.n_items]) return;
-    int lo = 0, hi = a.n_items - 1;
-    while (lo < hi) {
-        const int mid = (lo + hi + 1) >> 1;
-        if (a.ipre[mid] <= gi) lo = mid; else hi = mid - 1;
+    const int total = a.ipre[a.n_items];
+    for (int gi = blockIdx.x * blockDim.x + threadIdx.x; gi < total; gi += gridDim.x * blockDim.x) {
+        int lo = 0, hi = a.n_items - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (a.ipre[mid] <= gi) lo = mid; else hi = mid - 1;
+        }
+        const ForceParams &p = a.items[lo];
+        if (p.nsplit <= 1) continue;
+        const int i = gi - a.ipre[lo];
+        Partial q = p.part[i];
+        for (int s = 1; s < p.nsplit; ++s) add_partial(q, p.part[(size_t)s * p.ni + i]);
+        write_final(p, i, q);
     }
-    const ForceParams &p = a.items[lo];
-    if (p.nsplit <= 1) return;
-    const int i = gi - a.ipre[lo];
-    Partial q = p.part[i];
-    for (int s = 1; s < p.nsplit; ++s) add_partial(q, p.part[(size_t)s * p.ni + i]);
-    write_final(p, i, q);
 }
 
 __global__ void reduce_partials_kernel(const ForceParams p) {
@@ -916,7 +918,7 @@ cudaError_t launch_force_batch(cudaStream_t s, int kmode, const ForceConfig &cfg
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     if (total_i > 0) {
-        batch_reduce_kernel<<<(total_i + 255) / 256, 256, 0, s>>>(a);
+        batch_reduce_kernel<<<std::min((total_i + 255) / 256, 1184), 256, 0, s>>>(a);
         e = cudaGetLastError();
     }
     return e;
