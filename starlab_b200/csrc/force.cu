@@ -744,8 +744,19 @@ __global__ void __launch_bounds__(256, MinBlocks<K, R>::value) batch_force_kerne
         }
         const ForceParams p = a.items[lo];
         const int local = task - a.task0[lo];
-        const int n_itiles = (p.ni + itile - 1) / itile;
-        process_task<K, IL, R, NB, IDENT, V>(p, local % n_itiles, local / n_itiles, smem, gt);
+        const int il = batch_il(p.ni);  // the item's lane shape (its H is in p.H)
+        if (il == 32) {
+            const int n_itiles = (p.ni + itile - 1) / itile;
+            process_task<K, IL, R, NB, IDENT, V>(p, local % n_itiles, local / n_itiles, smem, gt);
+        } else if (il == 8) {
+            const int it8 = (blockDim.x >> 5) / p.H * 8;
+            const int n_itiles = (p.ni + it8 - 1) / it8;
+            process_task<K, 8, 1, NB, IDENT, V>(p, local % n_itiles, local / n_itiles, smem, gt);
+        } else {
+            const int it1 = (blockDim.x >> 5) / p.H;
+            const int n_itiles = (p.ni + it1 - 1) / it1;
+            process_task<K, 1, 1, NB, IDENT, V>(p, local % n_itiles, local / n_itiles, smem, gt);
+        }
     }
 }
 

@@ -121,15 +121,34 @@ __host__ __device__ inline int batch_itile(const ForceConfig &cfg) { return cfg.
 
 __host__ __device__ inline int tile_of(int kmode) { return kmode == kKernF64 ? 128 : 256; }
 
+// Lane shape of one item of a batched launch, from its own ni: blocks of
+// 1-2 i run one i per warp group with 32 j-lanes (IL = 1), blocks of up to
+// 16 run 8 i-lanes x 4 j-lanes (IL = 8) with every warp on the j-range, and
+// larger ones the launch's IL = 32 shape -- so a small block does not leave
+// most of a 32-lane i-tile idle.
+__host__ __device__ inline int batch_il(int ni) { return ni <= 2 ? 1 : (ni <= 16 ? 8 : 32); }
+__host__ __device__ inline int batch_item_H(int kmode, const ForceConfig &cfg, int ni) {
+    const int il = batch_il(ni);
+    if (il == 32) return cfg.H;
+    const int units = kmode == kKernMixedP ? tile_of(kmode) / 2 : tile_of(kmode);  // records per tile
+    int h = cfg.warps;
+    while (h > 1 && units / (h * (32 / il)) < 1) h /= 2;  // at least one record per lane per tile
+    return h;
+}
+__host__ __device__ inline int batch_item_itile(int kmode, const ForceConfig &cfg, int ni) {
+    const int il = batch_il(ni);
+    return il == 32 ? batch_itile(cfg) : cfg.warps / batch_item_H(kmode, cfg, ni) * il;
+}
+
 // Split rule of the batched kernel: a constant number of tasks wanted per
 // item (never the batch size), at least 4 tiles per split.
 __host__ __device__ inline void batch_plan(int kmode, const ForceConfig &cfg, ForceParams &item, int &n_tasks) {
     const int kTargetTasks = 592;
     const int T = tile_of(kmode);
     const int ntiles = item.nj_pad / T;
-    const int itile = batch_itile(cfg);
+    const int itile = batch_item_itile(kmode, cfg, item.ni);
     const int n_itiles = (item.ni + itile - 1) / itile;
-    item.H = cfg.H;
+    item.H = batch_item_H(kmode, cfg, item.ni);
     if (item.ni <= 0) {
         item.nsplit = 1;
         item.jper = T;

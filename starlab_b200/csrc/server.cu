@@ -440,10 +440,20 @@ int Server::run_batch(Lane &L, std::vector<std::shared_ptr<Request>> &batch) {
     const int T = tile_of(kmode_);
     const size_t rec = kmode_ == kKernF64 ? sizeof(JRecF64) : sizeof(JRecMixed);
     size_t ni_total = 0, parts = 0, jbytes = 0;
+    // Split partials by each call's own plan (batch_plan depends on the
+    // call's ni and nj only), so that large i-blocks -- one split -- need none.
+    auto split_of = [&](const Request &r) {
+        ForceParams q{};
+        q.ni = r.ni;
+        q.nj_pad = (r.nj + T - 1) / T * T;
+        int nt = 0;
+        batch_plan(kmode_, cfg_, q, nt);
+        return q.nsplit > 1 ? (size_t)q.nsplit : 0;
+    };
     for (auto &r : batch) {
         const int nj_pad = (r->nj + T - 1) / T * T;
         ni_total += r->ni;
-        parts += (size_t)r->ni * batch_max_split(kmode_, nj_pad);
+        parts += (size_t)r->ni * split_of(*r);
         jbytes += (size_t)nj_pad * rec;
     }
     if (ensure(L, std::max<size_t>(ni_total, 1), std::max<size_t>(parts, 1), std::max<size_t>(jbytes, 256), nb))
@@ -503,7 +513,7 @@ int Server::run_batch(Lane &L, std::vector<std::shared_ptr<Request>> &batch) {
         L.h_pre[nb + 1 + k] = (int)ioff;
         task += nt;
         ioff += r.ni;
-        poff += (size_t)r.ni * batch_max_split(kmode_, nj_pad);
+        poff += (size_t)r.ni * (p.nsplit > 1 ? (size_t)p.nsplit : 0);
         joff += (size_t)nj_pad * rec;
     }
     L.h_pre[nb] = task;
