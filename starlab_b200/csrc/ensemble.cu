@@ -56,6 +56,7 @@ struct EnsDev {
     Partial *part;
     ForceParams *items;
     int *task0, *ipre, *counter;
+    int *tcnt;  // per-particle slots of i-tile arrival counters (split reduction in the force kernel)
     unsigned *status;
     int *active;
     unsigned long long *interactions;
@@ -77,39 +78,56 @@ __device__ __forceinline__ void predict_state(const EnsDev &d, int g, double tb,
 
 // mode 0: next block; mode 1: every particle at its current time (start of
 // the run, or an energy evaluation when all times are equal).
-__global__ void __launch_bounds__(256) ens_schedule_kernel(EnsDev d, int mode) {
-    __shared__ double s_wmin[8];
-    __shared__ int s_wcnt[8];
+// One CTA of 1024 threads per cluster.  Each step takes kSchedPer x 1024
+// consecutive particles (element k of a thread: base + k*1024 + tid, so
+// loads are coalesced) and gives every block member its ordered slot.
+constexpr int kSchedThreads = 1024;
+constexpr int kSchedPer = 4;
+
+__global__ void __launch_bounds__(kSchedThreads) ens_schedule_kernel(EnsDev d, int mode) {
+    constexpr int NW = kSchedThreads / 32;
+    __shared__ double s_wmin[NW];
+    __shared__ int s_wcnt[kSchedPer][NW];
     const int c = blockIdx.x, tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
     const int n = d.n[c], o = d.off[c], span = d.off[c + 1] - o;  // span: n padded to 256
     double tmin = DBL_MAX;
     if (mode == 0)
-        for (int i = tid; i < n; i += 256) tmin = fmin(tmin, d.t[o + i] + d.dt[o + i]);
+        for (int i = tid; i < n; i += kSchedThreads) tmin = fmin(tmin, d.t[o + i] + d.dt[o + i]);
 #pragma unroll
     for (int k = 16; k > 0; k >>= 1) tmin = fmin(tmin, __shfl_xor_sync(0xffffffffu, tmin, k));
     if (lane == 0) s_wmin[w] = tmin;
     __syncthreads();
-    for (int k = 0; k < 8; ++k) tmin = fmin(tmin, s_wmin[k]);
+    for (int k = 0; k < NW; ++k) tmin = fmin(tmin, s_wmin[k]);
     const double tb = mode == 0 ? tmin : (n > 0 ? d.t[o] : 0.0);
     const bool active = n > 0 && (mode != 0 || tb <= d.t_end);
-    // Ordered compaction of the block members, 256 particles per step
-    // (coalesced): slot = members before this particle in address order.
+    // Ordered compaction of the block members: slot = members before this
+    // particle in address order.
     int running = 0;
-    for (int base = 0; base < span; base += 256) {
-        const int i = base + tid;
-        const bool mem = i < n && active && (mode != 0 || d.t[o + i] + d.dt[o + i] == tb);
-        const unsigned bal = __ballot_sync(0xffffffffu, mem);
-        if (lane == 0) s_wcnt[w] = __popc(bal);
-        __syncthreads();
-        int woff = 0, tot = 0;
+    for (int base = 0; base < span; base += kSchedPer * kSchedThreads) {
+        bool mem[kSchedPer];
+        unsigned bal[kSchedPer];
 #pragma unroll
-        for (int k = 0; k < 8; ++k) {
-            const int v = s_wcnt[k];
-            woff += k < w ? v : 0;
-            tot += v;
+        for (int k = 0; k < kSchedPer; ++k) {
+            const int i = base + k * kSchedThreads + tid;
+            mem[k] = i < n && active && (mode != 0 || d.t[o + i] + d.dt[o + i] == tb);
+            bal[k] = __ballot_sync(0xffffffffu, mem[k]);
+            if (lane == 0) s_wcnt[k][w] = __popc(bal[k]);
         }
-        d.slot[o + i] = mem ? running + woff + __popc(bal & ((1u << lane) - 1u)) : -1;
-        running += tot;
+        __syncthreads();
+        int before = running;  // members of the earlier sub-steps and warps
+#pragma unroll
+        for (int k = 0; k < kSchedPer; ++k) {
+            int woff = 0, tot = 0;
+            for (int q = 0; q < NW; ++q) {
+                const int v = s_wcnt[k][q];
+                woff += q < w ? v : 0;
+                tot += v;
+            }
+            const int i = base + k * kSchedThreads + tid;
+            if (i < span) d.slot[o + i] = mem[k] ? before + woff + __popc(bal[k] & ((1u << lane) - 1u)) : -1;
+            before += tot;
+        }
+        running = before;
         __syncthreads();
     }
     if (tid == 0) {
@@ -131,6 +149,7 @@ __global__ void __launch_bounds__(256) ens_schedule_kernel(EnsDev d, int mode) {
         p.out_pot = d.pot1 + o;
         p.out_nn = d.nn1 + o;
         p.status = d.status;
+        p.tile_counter = d.tcnt + o;  // n_itiles <= ni <= n: the last CTA of an i-tile adds its splits
         int nt = 0;
         batch_plan(d.kmode, d.cfg, p, nt);
         d.items[c] = p;
@@ -534,6 +553,7 @@ int Ensemble::setup() {
     ECHK(alloc(&p, sizeof(int) * (nc_ + 1)), "alloc"); d_.task0 = (int *)p;
     ECHK(alloc(&p, sizeof(int) * (nc_ + 1)), "alloc"); d_.ipre = (int *)p;
     ECHK(alloc(&p, sizeof(int) * 4), "alloc"); d_.counter = (int *)p;
+    ECHK(alloc(&p, sizeof(int) * N), "alloc"); d_.tcnt = (int *)p;
     ECHK(alloc(&p, sizeof(unsigned) * 4), "alloc"); d_.status = (unsigned *)p;
     ECHK(alloc(&p, sizeof(int) * 4), "alloc"); d_.active = (int *)p;
     ECHK(alloc(&p, sizeof(unsigned long long) * 2), "alloc"); d_.interactions = (unsigned long long *)p;
@@ -599,7 +619,7 @@ int Ensemble::push_host_state() {
 }
 
 int Ensemble::iteration(int mode) {
-    ens_schedule_kernel<<<nc_, 256, 0, stream_>>>(d_, mode);
+    ens_schedule_kernel<<<nc_, kSchedThreads, 0, stream_>>>(d_, mode);
     ens_scan_kernel<<<1, 1024, 0, stream_>>>(d_);
     const int per = kmode_ == kKernMixedP ? 2 : 1;
     const int units = (ntot_ / per + 255) / 256;
@@ -612,7 +632,8 @@ int Ensemble::iteration(int mode) {
     ba.H = d_.cfg.H;
     ba.counter = d_.counter;
     ba.one_task_per_cta = 0;
-    cudaError_t e = launch_force_batch(stream_, kmode_, d_.cfg, ba, ctas_, ntot_, false, true);
+    // total_i = 0: the splits are folded inside the force kernel (tile_counter)
+    cudaError_t e = launch_force_batch(stream_, kmode_, d_.cfg, ba, ctas_, 0, false, true);
     if (e != cudaSuccess) return fail("force launch", e);
     if (mode != 2) ens_correct_kernel<<<4 * num_sms_, 256, 0, stream_>>>(d_, mode);
     return cudaGetLastError() == cudaSuccess ? 0 : -1;

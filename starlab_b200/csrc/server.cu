@@ -96,6 +96,7 @@ struct Lane {
     ForceParams *h_items = nullptr, *d_items = nullptr;
     int *h_pre = nullptr, *d_pre = nullptr;
     int *d_counter = nullptr;
+    int *d_tcnt = nullptr;  // [cap_i] i-tile arrival counters, zero between batches
     std::vector<void *> retired_host;  // pinned buffers replaced by larger ones (freed at shutdown)
 };
 
@@ -209,7 +210,7 @@ void Server::free_lane(Lane &L) {
     if (L.h_items) cudaFreeHost(L.h_items);
     if (L.h_pre) cudaFreeHost(L.h_pre);
     for (void *p : {(void *)L.d_irec, (void *)L.d_out, (void *)L.d_part, (void *)L.d_items, (void *)L.d_pre,
-                    (void *)L.d_jrec})
+                    (void *)L.d_jrec, (void *)L.d_tcnt})
         if (p) cudaFreeAsync(p, L.stream);
     if (L.d_counter) cudaFree(L.d_counter);
     if (L.stream) cudaStreamSynchronize(L.stream);
@@ -403,7 +404,9 @@ int Server::ensure(Lane &L, size_t ni_total, size_t parts, size_t jrec_bytes, in
     if (ni_total > L.cap_i) {
         size_t n = std::max(ni_total, L.cap_i * 2);
         if (!host_realloc(L.h_irec, sizeof(IRec) * n) || !dev_realloc(L.d_irec, sizeof(IRec) * n) ||
-            !host_realloc(L.h_out, 16 + 60 * n) || !dev_realloc(L.d_out, 16 + 60 * n))
+            !host_realloc(L.h_out, 16 + 60 * n) || !dev_realloc(L.d_out, 16 + 60 * n) ||
+            !dev_realloc(L.d_tcnt, sizeof(int) * n) ||
+            cudaMemsetAsync(L.d_tcnt, 0, sizeof(int) * n, L.stream) != cudaSuccess)
             return -1;
         L.cap_i = n;
     }
@@ -506,6 +509,7 @@ int Server::run_batch(Lane &L, std::vector<std::shared_ptr<Request>> &batch) {
         p.out_pot = opot + ioff;
         p.out_nn = onn + ioff;
         p.status = d_status;
+        p.tile_counter = L.d_tcnt + ioff;  // the last CTA of an i-tile adds its splits
         int nt = 0;
         batch_plan(kmode_, cfg_, p, nt);
         L.h_items[k] = p;
@@ -534,7 +538,7 @@ int Server::run_batch(Lane &L, std::vector<std::shared_ptr<Request>> &batch) {
     a.one_task_per_cta = L.persistent ? 0 : 1;
     cudaError_t e = cudaSuccess;
     if (task > 0)
-        e = launch_force_batch(L.stream, kmode_, cfg_, a, L.persistent ? ctas_ : task, (int)ni_total, false, ident);
+        e = launch_force_batch(L.stream, kmode_, cfg_, a, L.persistent ? ctas_ : task, 0, false, ident);
     if (e != cudaSuccess) return -3;
     cudaMemcpyAsync(L.h_out, L.d_out, 16 + 60 * ni_total, cudaMemcpyDeviceToHost, L.stream);
     cudaEventRecord(L.ev_t1, L.stream);
@@ -542,6 +546,12 @@ int Server::run_batch(Lane &L, std::vector<std::shared_ptr<Request>> &batch) {
     float ms = 0;
     cudaEventElapsedTime(&ms, L.ev_t0, L.ev_t1);
     const unsigned status = *reinterpret_cast<unsigned *>(L.h_out);
+    if (status & ST_TMA_TIMEOUT) {  // results invalid; a task may have left its counter raised
+        cudaMemsetAsync(L.d_tcnt, 0, sizeof(int) * L.cap_i, L.stream);
+        cudaStreamSynchronize(L.stream);
+        err = "server: j-tile copy wait timed out on the device";
+        return -5;
+    }
     long long inter = 0;
     if (status & ST_RANGE) {
         // rare: redo each call alone with a widened fixed-point range
