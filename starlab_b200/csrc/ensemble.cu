@@ -78,11 +78,13 @@ __device__ __forceinline__ void predict_state(const EnsDev &d, int g, double tb,
 
 // mode 0: next block; mode 1: every particle at its current time (start of
 // the run, or an energy evaluation when all times are equal).
-// One CTA of 1024 threads per cluster.  Each step takes kSchedPer x 1024
-// consecutive particles (element k of a thread: base + k*1024 + tid, so
-// loads are coalesced) and gives every block member its ordered slot.
-constexpr int kSchedThreads = 1024;
-constexpr int kSchedPer = 4;
+// One CTA of 512 threads per cluster.  Each step covers kSchedPer x 512
+// particles, element k of a thread at base + k * 512 + tid (coalesced);
+// all of a step's loads are issued before any of them is used, so a large
+// cluster keeps enough bytes in flight (the kernel is latency-bound
+// otherwise: one CTA walks up to 16384 particles).
+constexpr int kSchedThreads = 512;
+constexpr int kSchedPer = 8;
 
 __global__ void __launch_bounds__(kSchedThreads) ens_schedule_kernel(EnsDev d, int mode) {
     constexpr int NW = kSchedThreads / 32;
@@ -90,9 +92,20 @@ __global__ void __launch_bounds__(kSchedThreads) ens_schedule_kernel(EnsDev d, i
     __shared__ int s_wcnt[kSchedPer][NW];
     const int c = blockIdx.x, tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
     const int n = d.n[c], o = d.off[c], span = d.off[c + 1] - o;  // span: n padded to 256
+    const double *t = d.t + o, *dt = d.dt + o;
     double tmin = DBL_MAX;
-    if (mode == 0)
-        for (int i = tid; i < n; i += kSchedThreads) tmin = fmin(tmin, d.t[o + i] + d.dt[o + i]);
+    if (mode == 0) {
+        for (int base = 0; base < n; base += kSchedPer * kSchedThreads) {
+            double tn[kSchedPer];
+#pragma unroll
+            for (int k = 0; k < kSchedPer; ++k) {
+                const int i = base + k * kSchedThreads + tid;
+                tn[k] = i < n ? t[i] + dt[i] : DBL_MAX;
+            }
+#pragma unroll
+            for (int k = 0; k < kSchedPer; ++k) tmin = fmin(tmin, tn[k]);
+        }
+    }
 #pragma unroll
     for (int k = 16; k > 0; k >>= 1) tmin = fmin(tmin, __shfl_xor_sync(0xffffffffu, tmin, k));
     if (lane == 0) s_wmin[w] = tmin;
@@ -104,13 +117,16 @@ __global__ void __launch_bounds__(kSchedThreads) ens_schedule_kernel(EnsDev d, i
     // particle in address order.
     int running = 0;
     for (int base = 0; base < span; base += kSchedPer * kSchedThreads) {
-        bool mem[kSchedPer];
-        unsigned bal[kSchedPer];
+        double tn[kSchedPer];
 #pragma unroll
         for (int k = 0; k < kSchedPer; ++k) {
             const int i = base + k * kSchedThreads + tid;
-            mem[k] = i < n && active && (mode != 0 || d.t[o + i] + d.dt[o + i] == tb);
-            bal[k] = __ballot_sync(0xffffffffu, mem[k]);
+            tn[k] = i < n ? t[i] + dt[i] : DBL_MAX;
+        }
+        unsigned bal[kSchedPer];
+#pragma unroll
+        for (int k = 0; k < kSchedPer; ++k) {
+            bal[k] = __ballot_sync(0xffffffffu, active && (mode != 0 ? base + k * kSchedThreads + tid < n : tn[k] == tb));
             if (lane == 0) s_wcnt[k][w] = __popc(bal[k]);
         }
         __syncthreads();
@@ -124,7 +140,8 @@ __global__ void __launch_bounds__(kSchedThreads) ens_schedule_kernel(EnsDev d, i
                 tot += v;
             }
             const int i = base + k * kSchedThreads + tid;
-            if (i < span) d.slot[o + i] = mem[k] ? before + woff + __popc(bal[k] & ((1u << lane) - 1u)) : -1;
+            if (i < span)
+                d.slot[o + i] = (bal[k] >> lane) & 1u ? before + woff + __popc(bal[k] & ((1u << lane) - 1u)) : -1;
             before += tot;
         }
         running = before;
