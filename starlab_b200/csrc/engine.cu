@@ -69,6 +69,7 @@ Engine::Engine(int cluster_id) : cluster_id_(cluster_id) {
     fault_lasthalf_at_ = env_ll("G6B200_FAULT_LASTHALF", -1);
     event_timing_ = getenv("G6B200_EVENT_TIMING") != nullptr;
     fault_pot_at_ = env_ll("G6B200_FAULT_POT", -1);
+    small_enabled_ = env_int("G6B200_SMALL_CALLS", 1) != 0;
 }
 
 Engine::~Engine() { close(); }
@@ -155,6 +156,11 @@ int Engine::reset() {
         cudaMemsetAsync(d_tile_cnt_, 0, sizeof(int) * call_cap_, stream_);
         cudaStreamSynchronize(stream_);
     }
+    if (d_out_) {
+        cudaMemsetAsync(d_out_, 0, 16, stream_);
+        cudaStreamSynchronize(stream_);
+    }
+    small_parity_ = 0;
     for (int k = 0; k < n_staged_; ++k) slot_of_[h_stage_addr_[k]] = -1;
     n_staged_ = 0;
     pending_ = false;
@@ -403,6 +409,8 @@ int Engine::ensure_call_buffers(int ni, bool nb, size_t part_bytes) {
         d_tile_cnt_ = nullptr;
         G6_CHECK(cudaMalloc(&d_tile_cnt_, sizeof(int) * ncap), "tile counters");
         G6_CHECK(cudaMemsetAsync(d_tile_cnt_, 0, sizeof(int) * ncap, stream_), "memset");
+        G6_CHECK(cudaMemsetAsync(d_out_, 0, 16, stream_), "memset");  // both status words clear
+        small_parity_ = 0;
         call_cap_ = ncap;
     }
     if (part_bytes > part_cap_) {
@@ -509,7 +517,8 @@ int Engine::firsthalf_impl(int nj, int ni, const int *index, const double (*xi)[
     call_copy_ = true;
     call_i0_ = 0;
     nb_read_ = false;
-    if (flush_j()) {
+    call_small_ = small_enabled_ && ni <= kSmallMax && n_staged_ <= kSmallMax;
+    if (!call_small_ && flush_j()) {
         call_error_ = true;
         return -1;
     }
@@ -537,10 +546,63 @@ int Engine::launch_call() {
     OutLayout L(ni);
     timed_ = event_timing_ || call_sweep_;
     if (timed_) G6_CHECK(cudaEventRecord(ev_begin_, stream_), "event");
-    G6_CHECK(cudaMemsetAsync(d_out_, 0, 16, stream_), "memset");
-    unsigned *status = reinterpret_cast<unsigned *>(d_out_ + L.status);
+    const bool small = call_small_ && !call_sweep_;
+    unsigned *status2 = reinterpret_cast<unsigned *>(d_out_ + L.status);
+    if (small) {
+        call_parity_ = small_parity_;
+        small_parity_ ^= 1;
+    } else {
+        G6_CHECK(cudaMemsetAsync(d_out_, 0, 16, stream_), "memset");
+        call_parity_ = 0;
+        small_parity_ = 1;  // word 1 stays clear: this call reports into word 0
+    }
+    unsigned *status = status2 + call_parity_;
     pred_timed_ = false;
-    if (!pred_valid_ || pred_ti_ != ti_ || pred_nj_ != nj || pred_mode_ != km || pred_E_ != E_) {
+    const bool need_pred = !pred_valid_ || pred_ti_ != ti_ || pred_nj_ != nj || pred_mode_ != km || pred_E_ != E_ ||
+                           (small && n_staged_ > 0);
+    if (small) {
+        // Updates, prediction and i-records in one launch whose parameter is
+        // the call's host data (no host->device copy).
+        SmallCall &sc = small_call_;
+        sc.n_upd = n_staged_;
+        sc.ni = ni;
+        sc.nj = nj;
+        sc.nj_pad = nj_pad;
+        sc.cap = cap_;
+        sc.predict = need_pred;
+        sc.parity = call_parity_;
+        sc.g4 = call_g4_;
+        sc.ti = ti_;
+        sc.fs = fs;
+        int order[kSmallMax];
+        for (int k = 0; k < n_staged_; ++k) order[k] = k;
+        std::sort(order, order + n_staged_, [&](int a, int b) { return h_stage_addr_[a] < h_stage_addr_[b]; });
+        for (int k = 0; k < n_staged_; ++k) {
+            const int sl = order[k];
+            sc.addr[k] = h_stage_addr_[sl];
+            sc.index[k] = h_stage_index_[sl];
+            memcpy(sc.vals[k], h_stage_vals_ + (size_t)sl * JF_COUNT, sizeof(double) * JF_COUNT);
+            slot_of_[h_stage_addr_[sl]] = -1;
+        }
+        memcpy(sc.irec, h_irec_, sizeof(IRec) * ni);
+        if (call_g4_) memcpy(sc.ieps2, h_ieps2_, sizeof(double) * ni);
+        stats_.h2d_bytes += (long long)sizeof(SmallCall);
+        n_staged_ = 0;
+        if (timed_) G6_CHECK(cudaEventRecord(ev_pred0_, stream_), "event");
+        launch_small_call(stream_, km, sc, d_jraw_, d_jindex_, d_jrec_, d_irec_, d_ieps2_, status2);
+        G6_CHECK(cudaGetLastError(), "small call launch");
+        stats_.launches++;
+        if (timed_) G6_CHECK(cudaEventRecord(ev_pred1_, stream_), "event");
+        pred_timed_ = need_pred;
+        if (need_pred) {
+            stats_.predictions++;
+            pred_valid_ = true;
+            pred_ti_ = ti_;
+            pred_nj_ = nj;
+            pred_mode_ = km;
+            pred_E_ = E_;
+        }
+    } else if (need_pred) {
         if (timed_) G6_CHECK(cudaEventRecord(ev_pred0_, stream_), "event");
         launch_predict(stream_, km, d_jraw_, d_jindex_, cap_, nj, nj_pad, ti_, fs, d_jrec_, status);
         G6_CHECK(cudaGetLastError(), "predict launch");
@@ -555,7 +617,9 @@ int Engine::launch_call() {
         pred_E_ = E_;
     }
     if (ni > 0) {
-        if (call_sweep_) {
+        if (small) {
+            // i-records (and softening) written by the small-call launch
+        } else if (call_sweep_) {
             launch_irec_from_j(stream_, d_jraw_, d_jindex_, cap_, call_i0_, ni, ti_, d_irec_);
             G6_CHECK(cudaGetLastError(), "i-record launch");
             stats_.launches++;
@@ -655,7 +719,7 @@ int Engine::wait_call() {
             fail("device execution", e);
             return 2;
         }
-        unsigned status = *reinterpret_cast<unsigned *>(h_out_);
+        unsigned status = reinterpret_cast<unsigned *>(h_out_)[call_parity_];
         if ((status & ST_RANGE) && attempt < 8) {
             // Fixed-point range exceeded: widen by 4x and recompute.
             stats_.range_retries++;
@@ -707,6 +771,7 @@ int Engine::sweep(int nj, int i0, int ni, double eps2, bool copy_out, double (*a
     call_eps2_ = eps2;
     call_nb_ = false;
     call_g4_ = false;
+    call_small_ = false;
     call_sweep_ = true;
     call_copy_ = copy_out;
     call_i0_ = i0;

@@ -183,6 +183,12 @@ class Engine {
     double call_eps2_ = 0;
     bool call_nb_ = false;
     bool call_g4_ = false;
+    // Small calls (<= kSmallMax i and staged j-updates): one launch carries
+    // the host data as its parameter (G6B200_SMALL_CALLS=0 turns it off).
+    bool small_enabled_ = true;
+    bool call_small_ = false;
+    int small_parity_ = 0;  // status word the next small call reports into
+    int call_parity_ = 0;   // status word of the call in flight
     bool call_error_ = false;
     bool call_sweep_ = false;
     bool call_copy_ = true;
@@ -197,6 +203,7 @@ class Engine {
     long long lasthalf_count_ = 0;
 
     EngineStats stats_;
+    SmallCall small_call_{};  // the parameter block of the last small call
 };
 
 }  // namespace g6

@@ -96,6 +96,27 @@ struct BulkJ {
     const int *addr, *index;
 };
 void launch_scatter_bulk(cudaStream_t s, int n, const BulkJ &b, double *jraw, int *jindex, int cap);
+// A small force call's host data, passed by value as the parameter of one
+// kernel (so a call of up to kSmallMax i-particles and j-updates needs no
+// host->device copy): the staged j-updates (ascending address), the
+// i-records, and the prediction to make.
+constexpr int kSmallMax = 64;
+struct SmallCall {
+    int n_upd, ni, nj, nj_pad, cap, predict, parity, g4;
+    double ti;
+    FixedScale fs;
+    int addr[kSmallMax];
+    int index[kSmallMax];
+    double vals[kSmallMax][JF_COUNT];  // JF_* fields, as the staging records
+    IRec irec[kSmallMax];
+    double ieps2[kSmallMax];           // GRAPE-4 calls
+};
+// One launch: apply the updates to the raw j-state, predict j (if
+// sc.predict) into jrec, write the i-records (and GRAPE-4 softening), and
+// clear status word parity ^ 1 for the next call; range reports go to word
+// parity.
+void launch_small_call(cudaStream_t s, int kmode, const SmallCall &sc, double *jraw, int *jindex, void *jrec,
+                       IRec *irec, double *ieps2, unsigned *status2);
 void launch_predict(cudaStream_t s, int kmode, const double *jraw, const int *jindex, int cap,
                     int nj, int nj_pad, double ti, const FixedScale &fs, void *jrec,
                     unsigned *status);

@@ -176,6 +176,159 @@ __global__ void irec_from_j_kernel(const double *__restrict__ jraw, const int *_
     out[k] = r;
 }
 
+// ---- small calls: updates + prediction + i-records in one launch
+
+__device__ __forceinline__ void predict_vals(const double *v17, double ti, double xp[3], double vp[3], double &m) {
+    const double dt = ti - v17[JF_T];
+    m = v17[JF_M];
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+        const double x = v17[JF_X + c], v = v17[JF_V + c], a2 = v17[JF_A2 + c], j6 = v17[JF_J6 + c];
+        xp[c] = x + dt * (v + dt * (a2 + dt * j6));
+        vp[c] = v + dt * (2.0 * a2 + dt * (3.0 * j6));
+    }
+}
+
+// Position of address j in the ascending update list, or -1.
+__device__ __forceinline__ int find_update(const int *addr, int n, int j) {
+    int lo = 0, hi = n - 1;
+    while (lo <= hi) {
+        const int mid = (lo + hi) >> 1;
+        const int a = addr[mid];
+        if (a == j) return mid;
+        if (a < j) lo = mid + 1; else hi = mid - 1;
+    }
+    return -1;
+}
+
+// Predicted j (or a dummy beyond nj): the update's values when j is being
+// updated (its raw state is rewritten by another thread of this launch),
+// the raw j-state otherwise.
+__device__ __forceinline__ bool small_pred(const SmallCall &sc, const int *s_addr, const double *jraw,
+                                           const int *jindex, int j, double xp[3], double vp[3], double &m,
+                                           int &id) {
+    if (j >= sc.nj) return false;
+    const int s = find_update(s_addr, sc.n_upd, j);
+    if (s >= 0) {
+        predict_vals(sc.vals[s], sc.ti, xp, vp, m);
+        id = sc.index[s];
+    } else {
+        predict_one(jraw, sc.cap, j, sc.ti, xp, vp, m);
+        id = jindex[j];
+    }
+    return true;
+}
+
+template <int KM>
+__global__ void __launch_bounds__(256) small_call_kernel(const __grid_constant__ SmallCall sc,
+                                                         double *__restrict__ jraw, int *__restrict__ jindex,
+                                                         void *__restrict__ jrec, IRec *__restrict__ irec,
+                                                         double *__restrict__ ieps2, unsigned *__restrict__ status2) {
+    __shared__ int s_addr[kSmallMax];
+    const int tid = threadIdx.x;
+    if (tid < sc.n_upd) s_addr[tid] = sc.addr[tid];
+    if (blockIdx.x == 0) {
+        if (tid < sc.ni) {
+            irec[tid] = sc.irec[tid];
+            if (sc.g4) ieps2[tid] = sc.ieps2[tid];
+        }
+        if (tid == 0) status2[sc.parity ^ 1] = 0u;
+        if (tid < sc.n_upd) {  // persist the updates (no thread of this launch reads these addresses' raw state)
+            const int a = sc.addr[tid];
+#pragma unroll
+            for (int f = 0; f < JF_COUNT; ++f) jraw[(size_t)f * sc.cap + a] = sc.vals[tid][f];
+            jindex[a] = sc.index[tid];
+        }
+    }
+    __syncthreads();
+    if (!sc.predict) return;
+    const int q = blockIdx.x * blockDim.x + tid;
+    if constexpr (KM == kKernF64) {
+        const int j = q;
+        if (j >= sc.nj_pad) return;
+        JRecF64 r;
+        double xp[3], vp[3], m;
+        int id;
+        if (small_pred(sc, s_addr, jraw, jindex, j, xp, vp, m, id)) {
+            r.pos = make_double4(xp[0], xp[1], xp[2], m);
+            r.vel = make_double4(vp[0], vp[1], vp[2], (double)id);
+        } else {
+            r.pos = make_double4(kDummyPos, kDummyPos, kDummyPos, 0.0);
+            r.vel = make_double4(0.0, 0.0, 0.0, -1.0);
+        }
+        reinterpret_cast<JRecF64 *>(jrec)[j] = r;
+    } else if constexpr (KM == kKernMixedDS) {
+        const int j = q;
+        if (j >= sc.nj_pad) return;
+        JRecMixed r;
+        double xp[3], vp[3], m;
+        int id;
+        if (small_pred(sc, s_addr, jraw, jindex, j, xp, vp, m, id)) {
+            float hi[3], lo[3];
+            bool bad = false;
+#pragma unroll
+            for (int c = 0; c < 3; c++) bad |= !to_fixed_split(xp[c], sc.fs, hi[c], lo[c]);
+            if (bad) atomicOr(&status2[sc.parity], ST_RANGE);
+            r.hi = make_float4(hi[0], hi[1], hi[2], (float)m);
+            r.lo = make_float4(lo[0], lo[1], lo[2], __int_as_float(id));
+            r.vel = make_float4((float)vp[0], (float)vp[1], (float)vp[2], 0.f);
+        } else {
+            r.hi = make_float4(kDummyPos, kDummyPos, kDummyPos, 0.f);
+            r.lo = make_float4(0.f, 0.f, 0.f, __int_as_float(-1));
+            r.vel = make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+        reinterpret_cast<JRecMixed *>(jrec)[j] = r;
+    } else {
+        if (2 * q >= sc.nj_pad) return;
+        float hi[2][3], lo[2][3], v[2][3], m[2];
+        int id[2];
+        bool bad = false;
+#pragma unroll
+        for (int u = 0; u < 2; ++u) {
+            double xp[3], vp[3], mm;
+            if (small_pred(sc, s_addr, jraw, jindex, 2 * q + u, xp, vp, mm, id[u])) {
+#pragma unroll
+                for (int c = 0; c < 3; c++) {
+                    bad |= !to_fixed_split(xp[c], sc.fs, hi[u][c], lo[u][c]);
+                    v[u][c] = (float)vp[c];
+                }
+                m[u] = (float)mm;
+            } else {
+#pragma unroll
+                for (int c = 0; c < 3; c++) {
+                    hi[u][c] = kDummyPos;
+                    lo[u][c] = 0.f;
+                    v[u][c] = 0.f;
+                }
+                m[u] = 0.f;
+                id[u] = -1;
+            }
+        }
+        if (bad) atomicOr(&status2[sc.parity], ST_RANGE);
+        JPairMixed r;
+        r.hxy = make_float4(hi[0][0], hi[1][0], hi[0][1], hi[1][1]);
+        r.hzm = make_float4(hi[0][2], hi[1][2], -0.125f * m[0], -0.125f * m[1]);  // -m/8: see JPairMixed
+        r.lxy = make_float4(lo[0][0], lo[1][0], lo[0][1], lo[1][1]);
+        r.lzi = make_float4(lo[0][2], lo[1][2], __int_as_float(id[0]), __int_as_float(id[1]));
+        r.vxy = make_float4(v[0][0], v[1][0], v[0][1], v[1][1]);
+        r.vz = make_float4(v[0][2], v[1][2], 0.f, 0.f);
+        reinterpret_cast<JPairMixed *>(jrec)[q] = r;
+    }
+}
+
+void launch_small_call(cudaStream_t s, int kmode, const SmallCall &sc, double *jraw, int *jindex, void *jrec,
+                       IRec *irec, double *ieps2, unsigned *status2) {
+    const int per = kmode == kKernMixedP ? 2 : 1;
+    const int units = sc.predict ? (sc.nj_pad + per - 1) / per : 1;
+    const int blocks = (units + 255) / 256 > 0 ? (units + 255) / 256 : 1;
+    if (kmode == kKernF64)
+        small_call_kernel<kKernF64><<<blocks, 256, 0, s>>>(sc, jraw, jindex, jrec, irec, ieps2, status2);
+    else if (kmode == kKernMixedDS)
+        small_call_kernel<kKernMixedDS><<<blocks, 256, 0, s>>>(sc, jraw, jindex, jrec, irec, ieps2, status2);
+    else
+        small_call_kernel<kKernMixedP><<<blocks, 256, 0, s>>>(sc, jraw, jindex, jrec, irec, ieps2, status2);
+}
+
 void launch_irec_from_j(cudaStream_t s, const double *jraw, const int *jindex, int cap, int i0, int ni,
                         double ti, IRec *out) {
     if (ni <= 0) return;

@@ -172,3 +172,53 @@ def test_open_close_reset_cycles(oracle):
         ref = oracle.force(x, v, m, idx, x[:50], v[:50], 1e-6)
         assert rel_err_vec(got[0], ref[0]).max() < 1e-12
         e.close()
+
+
+@pytest.mark.parametrize("mode", ["fp64", "mixed"])
+def test_small_call_path_matches_copy_path(mode):
+    """Calls of <= 64 i with <= 64 staged j-updates run as one launch whose
+    parameter carries the updates and i-records (no host->device copies).
+    A kira-like sequence -- block updates, new block time, firsthalf /
+    lasthalf2, a second chunk at the same time, a neighbour-list call --
+    gives bit-identical results with that path switched off
+    (G6B200_SMALL_CALLS=0), and the j-memory it leaves behind is the same."""
+    import os
+    from starlab_b200 import G6Engine
+    n = 3000
+    m, x, v, a, j = snapshot(n, 31)
+    rng = np.random.default_rng(7)
+    outs = []
+    for small in ("1", "0"):
+        os.environ["G6B200_SMALL_CALLS"] = small
+        try:
+            e = eng(mode, npipes=64)
+        finally:
+            os.environ.pop("G6B200_SMALL_CALLS", None)
+        e.set_j_particles(0.0, m, j / 6.0, 0.5 * a, v, x)
+        res = []
+        rr = np.random.default_rng(7)
+        for blk in range(12):
+            upd = np.sort(rr.choice(n, 40 if blk % 3 else 64, replace=False))
+            for q in upd:
+                e.set_j_particle(int(q), 1e-3 * blk, m[q], np.zeros(3), (j / 6.0)[q], (0.5 * a)[q], v[q],
+                                 x[q] * (1 + 1e-4 * blk))
+            e.set_ti(1e-3 * (blk + 1))
+            ii = np.sort(rr.choice(n, 64, replace=False)).astype(np.int32)
+            res.append(e.force(n, ii, x[ii], v[ii], 1e-6))
+            res.append(e.force(n, ii[:17], x[ii[:17]] * 1.0001, v[ii[:17]], 1e-6))   # same time, no updates
+            h2 = np.full(9, 0.01)
+            e.calc_firsthalf(n, ii[:9], x[ii[:9]], v[ii[:9]], 1e-6, h2)
+            res.append(e.calc_lasthalf2())
+            e.read_neighbour_list()
+            res.append(tuple(e.get_neighbour_list(k) for k in range(9)))
+        res.append(e.sweep(n, eps2=1e-6))   # the j-memory after all updates
+        outs.append(res)
+        e.close()
+    def same(p, q):
+        if isinstance(p, (tuple, list)):
+            return len(p) == len(q) and all(same(u, w) for u, w in zip(p, q))
+        return np.array_equal(np.asarray(p), np.asarray(q))
+
+    assert len(outs[0]) == len(outs[1])
+    for k, (r1, r2) in enumerate(zip(*outs)):
+        assert same(r1, r2), k
