@@ -51,7 +51,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(HERE)
 OUT = os.path.join(HERE, "_ref")
 
-# Directories whose libtool convenience libraries kira links (SURVEY-verified set).
+# Directories whose libtool convenience libraries kira links (the set its Makefile.am files name).
 LIB_DIRS = [
     "std", "node/util", "node/dyn/util", "node/dyn/kepler", "node/dyn/init",
     "node/dyn/evolve", "node/dyn/_dyn_", "node/dyn/hdyn/util",
