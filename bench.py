@@ -185,6 +185,7 @@ def ensemble_section(nc, t_full, seed):
     out["batched_full"] = {"t_end": t_full, "seconds": st["seconds"], "interactions": st["interactions"],
                            "interactions_per_s": st["interactions"] / st["seconds"],
                            "iterations": st["iterations"], "tuned_i_tile": 256 // st["tuned_h"],
+                           "tuned_tasks_per_cluster": st["tuned_tasks"],
                            "dE_over_E_median": float(np.median(de)), "dE_over_E_max": float(de.max())}
     slice_t = 1.0 / 64
     for key, per in (("batched_slice", False), ("per_cluster_slice", True)):

@@ -212,6 +212,7 @@ typedef struct {
     long long iterations;
     long long launches;
     int tuned_h;
+    int tuned_tasks;     /* j-split factor chosen by the tuner (tasks wanted per cluster) */
 } g6b200_ens_stats;
 g6b200_ensemble *g6b200_ens_create(int nclusters, const int *n, const double *eps2, double eta,
                                    int precision, int device);

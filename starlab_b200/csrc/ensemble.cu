@@ -447,6 +447,7 @@ struct EnsembleStats {
     long long iterations = 0;
     long long launches = 0;
     double tuned_h = 0;
+    int tuned_tasks = 0;
 };
 
 class Ensemble {
@@ -678,36 +679,48 @@ int Ensemble::run_batched(double t_end, EnsembleStats *st, int tune) {
     ECHK(cudaStreamSynchronize(stream_), "cap");
     auto t0 = std::chrono::steady_clock::now();
     long long iters = 0;
-    // Autotune the i-tile (H warps per j-tile) on the first iterations.
+    // Autotune the launch shape on the first iterations of the run: the
+    // i-tile of large blocks (H warps per j-tile: i per CTA = 256 / H) and
+    // the j-split factor (tasks wanted per cluster), by measured time per
+    // iteration on the live integration.
     if (tune) {
-        const int cands[4] = {8, 4, 2, 1};
+        const int hs[4] = {8, 4, 2, 1};
+        const int targets[3] = {296, 592, 1184};
         double best = 1e30;
-        int bestH = d_.cfg.H;
+        int bestH = d_.cfg.H, bestT = d_.cfg.nsplit;
         cudaEvent_t e0, e1;
         cudaEventCreate(&e0);
         cudaEventCreate(&e1);
-        for (int h : cands) {
-            d_.cfg.H = h;
-            ctas_ = batch_ctas(kmode_, d_.cfg, num_sms_);
-            cudaEventRecord(e0, stream_);
-            for (int k = 0; k < 16; ++k)
-                if (iteration(0)) return -1;
-            cudaEventRecord(e1, stream_);
-            cudaEventSynchronize(e1);
-            iters += 16;
-            float ms = 0;
-            cudaEventElapsedTime(&ms, e0, e1);
-            if (ms < best) {
-                best = ms;
-                bestH = h;
+        for (int tt : targets) {
+            for (int h : hs) {
+                d_.cfg.H = h;
+                d_.cfg.nsplit = tt;
+                ctas_ = batch_ctas(kmode_, d_.cfg, num_sms_);
+                cudaEventRecord(e0, stream_);
+                for (int k = 0; k < 8; ++k)
+                    if (iteration(0)) return -1;
+                cudaEventRecord(e1, stream_);
+                cudaEventSynchronize(e1);
+                iters += 8;
+                float ms = 0;
+                cudaEventElapsedTime(&ms, e0, e1);
+                if (ms < best) {
+                    best = ms;
+                    bestH = h;
+                    bestT = tt;
+                }
             }
         }
         cudaEventDestroy(e0);
         cudaEventDestroy(e1);
         d_.cfg.H = bestH;
+        d_.cfg.nsplit = bestT;
         ctas_ = batch_ctas(kmode_, d_.cfg, num_sms_);
     }
-    if (st) st->tuned_h = d_.cfg.H;
+    if (st) {
+        st->tuned_h = d_.cfg.H;
+        st->tuned_tasks = d_.cfg.nsplit > 0 ? d_.cfg.nsplit : 592;
+    }
     // Capture K iterations as one graph.
     const int K = 8;
     cudaGraph_t g;
@@ -1001,6 +1014,7 @@ __attribute__((visibility("default"))) int g6b200_ens_run(g6b200_ensemble *h, do
         out->iterations = st.iterations;
         out->launches = st.launches;
         out->tuned_h = (int)st.tuned_h;
+        out->tuned_tasks = st.tuned_tasks;
     }
     return 0;
 }

@@ -162,9 +162,10 @@ __host__ __device__ inline int batch_item_itile(int kmode, const ForceConfig &cf
 }
 
 // Split rule of the batched kernel: a constant number of tasks wanted per
-// item (never the batch size), at least 4 tiles per split.
+// item (never the batch size; cfg.nsplit when set, e.g. by the ensemble's
+// tuner, else 592 = 4 x 148), at least 4 tiles per split.
 __host__ __device__ inline void batch_plan(int kmode, const ForceConfig &cfg, ForceParams &item, int &n_tasks) {
-    const int kTargetTasks = 592;
+    const int kTargetTasks = cfg.nsplit > 0 ? cfg.nsplit : 592;
     const int T = tile_of(kmode);
     const int ntiles = item.nj_pad / T;
     const int itile = batch_item_itile(kmode, cfg, item.ni);
