@@ -517,7 +517,10 @@ int Engine::firsthalf_impl(int nj, int ni, const int *index, const double (*xi)[
     call_copy_ = true;
     call_i0_ = 0;
     nb_read_ = false;
-    call_small_ = small_enabled_ && ni <= kSmallMax && n_staged_ <= kSmallMax;
+    // The one-launch form pays for its 14 KB parameter block by replacing the
+    // staged updates' copies and scatter: without updates the copy path
+    // (status clear, prediction, i-record copy) is as fast.
+    call_small_ = small_enabled_ && n_staged_ > 0 && ni <= kSmallMax && n_staged_ <= kSmallMax;
     if (!call_small_ && flush_j()) {
         call_error_ = true;
         return -1;
