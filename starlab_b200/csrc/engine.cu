@@ -21,10 +21,29 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <thread>
 
 namespace g6 {
 
 namespace {
+
+// Host-side work of large uploads and i-blocks split over up to 8 threads
+// (single-threaded memory copies run at a fraction of the host's bandwidth).
+// f(lo, hi, t) handles [lo, hi) as thread t; returns when all are done.
+template <class F>
+void parallel_ranges(size_t n, size_t min_per_thread, F &&f) {
+    const size_t hw = std::max(1u, std::thread::hardware_concurrency());
+    const size_t nt = std::min<size_t>(std::min<size_t>(hw, 8), std::max<size_t>(1, n / min_per_thread));
+    if (nt <= 1) {
+        f(size_t(0), n, size_t(0));
+        return;
+    }
+    std::vector<std::thread> th;
+    th.reserve(nt - 1);
+    for (size_t t = 1; t < nt; ++t) th.emplace_back([&, t] { f(n * t / nt, n * (t + 1) / nt, t); });
+    f(size_t(0), n / nt, size_t(0));
+    for (auto &x : th) x.join();
+}
 
 int env_int(const char *name, int dflt) {
     const char *s = getenv(name);
@@ -126,7 +145,7 @@ void Engine::close() {
     dfree(d_irec_); dfree(d_out_); dfree(d_part_); dfree(d_tile_cnt_);
     dfree(d_nb_count_); dfree(d_nb_list_); dfree(d_nb_sorted_); dfree(d_nb_off_); dfree(d_bulk_);
     hfree(h_stage_vals_); hfree(h_stage_addr_); hfree(h_stage_index_);
-    hfree(h_irec_); hfree(h_out_); hfree(h_nb_off_); hfree(h_nb_count_);
+    hfree(h_irec_); hfree(h_out_); hfree(h_nb_off_); hfree(h_nb_count_); hfree(h_bulk_);
     hfree(h_ieps2_); dfree(d_ieps2_);
     cudaEvent_t evs[] = {ev_stage_, ev_begin_, ev_pred0_, ev_pred1_, ev_force0_, ev_force1_, ev_done_};
     for (cudaEvent_t e : evs) if (e) cudaEventDestroy(e);
@@ -136,6 +155,7 @@ void Engine::close() {
     d_irec_ = nullptr; d_out_ = nullptr; d_part_ = nullptr; d_tile_cnt_ = nullptr;
     d_nb_count_ = nullptr; d_nb_list_ = nullptr; d_nb_sorted_ = nullptr; d_nb_off_ = nullptr;
     d_bulk_ = nullptr; bulk_cap_ = 0; bulk_mark_.clear();
+    h_bulk_ = nullptr; h_bulk_cap_ = 0; bulk_busy_ = false;
     h_stage_vals_ = nullptr; h_stage_addr_ = nullptr; h_stage_index_ = nullptr;
     h_irec_ = nullptr; h_out_ = nullptr; h_nb_off_ = nullptr; h_nb_count_ = nullptr;
     h_ieps2_ = nullptr; d_ieps2_ = nullptr;
@@ -331,33 +351,67 @@ int Engine::set_j_bulk(int n, const int *address, const int *index, const double
         G6_CHECK(cudaMalloc(&d_bulk_, bytes), "bulk j");
         bulk_cap_ = bytes;
     }
-    unsigned char *p = d_bulk_;
-    auto put = [&](const void *src, size_t b) -> const void * {
+    // The caller's arrays are gathered into one pinned block by a few host
+    // threads (and max |x| taken on the way), then sent in one copy.
+    if (bytes > h_bulk_cap_) {
+        if (h_bulk_) {
+            G6_CHECK(cudaEventSynchronize(ev_stage_), "bulk wait");
+            cudaFreeHost(h_bulk_);
+        }
+        h_bulk_ = nullptr;
+        h_bulk_cap_ = 0;
+        G6_CHECK(cudaMallocHost(&h_bulk_, bytes), "pinned bulk j");
+        h_bulk_cap_ = bytes;
+    } else if (bulk_busy_) {
+        G6_CHECK(cudaEventSynchronize(ev_stage_), "bulk wait");  // the previous bulk copy read h_bulk_
+    }
+    struct Part {
+        const void *src;
+        size_t bytes, off;
+    };
+    Part parts[9];
+    int np = 0;
+    size_t off = 0;
+    const void *dev[9];
+    auto add = [&](const void *src, size_t b) -> const void * {
         if (!src) return nullptr;
-        unsigned char *dst = p;
-        p += (b + 15) / 16 * 16;
-        return cudaMemcpyAsync(dst, src, b, cudaMemcpyHostToDevice, stream_) == cudaSuccess ? dst : nullptr;
+        parts[np++] = {src, b, off};
+        const void *d = d_bulk_ + off;
+        off += (b + 15) / 16 * 16;
+        return d;
     };
     BulkJ b;
-    b.t = static_cast<const double *>(put(tj, 8 * nd));
-    b.m = static_cast<const double *>(put(mass, 8 * nd));
-    b.x = static_cast<const double *>(put(x, vec));
-    b.v = static_cast<const double *>(put(v, vec));
-    b.a2 = static_cast<const double *>(put(a2, vec));
-    b.j6 = static_cast<const double *>(put(j6, vec));
-    b.k18 = static_cast<const double *>(put(k18, vec));
-    b.addr = static_cast<const int *>(put(address, 4 * nd));
-    b.index = static_cast<const int *>(put(index, 4 * nd));
-    if (!b.t || !b.m || !b.x || !b.v || !b.a2 || !b.j6 || (k18 && !b.k18) || (address && !b.addr) ||
-        (index && !b.index))
-        return fail("bulk j copy", cudaGetLastError());
+    b.t = static_cast<const double *>(add(tj, 8 * nd));
+    b.m = static_cast<const double *>(add(mass, 8 * nd));
+    b.x = static_cast<const double *>(add(x, vec));
+    b.v = static_cast<const double *>(add(v, vec));
+    b.a2 = static_cast<const double *>(add(a2, vec));
+    b.j6 = static_cast<const double *>(add(j6, vec));
+    b.k18 = static_cast<const double *>(add(k18, vec));
+    b.addr = static_cast<const int *>(add(address, 4 * nd));
+    b.index = static_cast<const int *>(add(index, 4 * nd));
+    (void)dev;
+    double tmax[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    parallel_ranges(nd, 16384, [&](size_t lo, size_t hi, size_t t) {
+        for (int k = 0; k < np; ++k) {
+            const size_t per = parts[k].bytes / nd;  // bytes per particle of this array
+            memcpy(h_bulk_ + parts[k].off + lo * per, static_cast<const unsigned char *>(parts[k].src) + lo * per,
+                   (hi - lo) * per);
+        }
+        double m = 0;
+        for (size_t q = 3 * lo; q < 3 * hi; ++q) m = std::max(m, std::fabs(x[q]));
+        tmax[t] = m;
+    });
+    G6_CHECK(cudaMemcpyAsync(d_bulk_, h_bulk_, off, cudaMemcpyHostToDevice, stream_), "bulk j copy");
+    G6_CHECK(cudaEventRecord(ev_stage_, stream_), "event");
+    bulk_busy_ = true;
     launch_scatter_bulk(stream_, n, b, d_jraw_, d_jindex_, cap_);
     G6_CHECK(cudaGetLastError(), "bulk scatter launch");
     stats_.launches++;
-    stats_.h2d_bytes += (long long)(p - d_bulk_);
+    stats_.h2d_bytes += (long long)off;
     stats_.j_updates += n;
     double xm = xmax_;
-    for (size_t k = 0; k < 3 * nd; ++k) xm = std::max(xm, std::fabs(x[k]));
+    for (double m : tmax) xm = std::max(xm, m);
     xmax_ = xm;
     for (int k = 0; k < n; ++k) {
         const int a = address ? address[k] : k;
@@ -493,20 +547,25 @@ int Engine::firsthalf_impl(int nj, int ni, const int *index, const double (*xi)[
         call_error_ = true;
         return -1;
     }
-    double xm = xmax_;
-    for (int i = 0; i < ni; ++i) {
-        IRec &r = h_irec_[i];
-        for (int c = 0; c < 3; ++c) {
-            r.x[c] = xi[i][c];
-            r.v[c] = vi[i][c];
-            double ax = std::fabs(xi[i][c]);
-            if (ax > xm) xm = ax;
+    double tmax[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    parallel_ranges((size_t)ni, 16384, [&](size_t lo, size_t hi, size_t t) {
+        double xm = 0;
+        for (size_t i = lo; i < hi; ++i) {
+            IRec &r = h_irec_[i];
+            for (int c = 0; c < 3; ++c) {
+                r.x[c] = xi[i][c];
+                r.v[c] = vi[i][c];
+                xm = std::max(xm, std::fabs(xi[i][c]));
+            }
+            r.h2 = h2 ? h2[i] : default_h2_;
+            r.index = index ? index[i] : -1;
+            r.pad = 0;
+            if (ieps2) h_ieps2_[i] = ieps2[i];
         }
-        r.h2 = h2 ? h2[i] : default_h2_;
-        r.index = index ? index[i] : -1;
-        r.pad = 0;
-        if (ieps2) h_ieps2_[i] = ieps2[i];
-    }
+        tmax[t] = xm;
+    });
+    double xm = xmax_;
+    for (double m : tmax) xm = std::max(xm, m);
     xmax_ = xm;
     call_ni_ = ni;
     call_nj_ = nj;
@@ -699,10 +758,12 @@ int Engine::lasthalf(int ni, double (*acc)[3], double (*jerk)[3], double *pot, i
     if (rc) return rc;
     const int n = std::min(ni, call_ni_);
     OutLayout L(call_ni_);
-    if (acc) memcpy(acc, h_out_ + L.acc, 24 * (size_t)n);
-    if (jerk) memcpy(jerk, h_out_ + L.jerk, 24 * (size_t)n);
-    if (pot) memcpy(pot, h_out_ + L.pot, 8 * (size_t)n);
-    if (nn) memcpy(nn, h_out_ + L.nn, 4 * (size_t)n);
+    parallel_ranges((size_t)n, 16384, [&](size_t lo, size_t hi, size_t) {
+        if (acc) memcpy(acc[lo], h_out_ + L.acc + 24 * lo, 24 * (hi - lo));
+        if (jerk) memcpy(jerk[lo], h_out_ + L.jerk + 24 * lo, 24 * (hi - lo));
+        if (pot) memcpy(pot + lo, h_out_ + L.pot + 8 * lo, 8 * (hi - lo));
+        if (nn) memcpy(nn + lo, h_out_ + L.nn + 4 * lo, 4 * (hi - lo));
+    });
     ++lasthalf_count_;
     if (fault_lasthalf_at_ >= 0 && lasthalf_count_ == fault_lasthalf_at_) {
         last_error = "g6b200: injected lasthalf failure (G6B200_FAULT_LASTHALF)";

@@ -154,6 +154,9 @@ class Engine {
     cudaEvent_t ev_stage_ = nullptr;
     unsigned char *d_bulk_ = nullptr;  // device copies of a bulk upload's arrays
     size_t bulk_cap_ = 0;
+    unsigned char *h_bulk_ = nullptr;  // pinned gather buffer of a bulk upload
+    size_t h_bulk_cap_ = 0;
+    bool bulk_busy_ = false;           // ev_stage_ marks the end of its last copy
     std::vector<unsigned> bulk_mark_;  // duplicate-address check (generation stamps)
     unsigned bulk_gen_ = 0;
     bool stage_busy_ = false;
