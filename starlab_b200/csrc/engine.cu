@@ -30,6 +30,8 @@ namespace {
 // Host-side work of large uploads and i-blocks split over up to 8 threads
 // (single-threaded memory copies run at a fraction of the host's bandwidth).
 // f(lo, hi, t) handles [lo, hi) as thread t; returns when all are done.
+// Threads are started per use, so callers ask for one only per
+// min_per_thread items (tens of thousands): starting one costs tens of us.
 template <class F>
 void parallel_ranges(size_t n, size_t min_per_thread, F &&f) {
     const size_t hw = std::max(1u, std::thread::hardware_concurrency());
@@ -548,7 +550,7 @@ int Engine::firsthalf_impl(int nj, int ni, const int *index, const double (*xi)[
         return -1;
     }
     double tmax[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-    parallel_ranges((size_t)ni, 16384, [&](size_t lo, size_t hi, size_t t) {
+    parallel_ranges((size_t)ni, 65536, [&](size_t lo, size_t hi, size_t t) {
         double xm = 0;
         for (size_t i = lo; i < hi; ++i) {
             IRec &r = h_irec_[i];
@@ -758,7 +760,7 @@ int Engine::lasthalf(int ni, double (*acc)[3], double (*jerk)[3], double *pot, i
     if (rc) return rc;
     const int n = std::min(ni, call_ni_);
     OutLayout L(call_ni_);
-    parallel_ranges((size_t)n, 16384, [&](size_t lo, size_t hi, size_t) {
+    parallel_ranges((size_t)n, 65536, [&](size_t lo, size_t hi, size_t) {
         if (acc) memcpy(acc[lo], h_out_ + L.acc + 24 * lo, 24 * (hi - lo));
         if (jerk) memcpy(jerk[lo], h_out_ + L.jerk + 24 * lo, 24 * (hi - lo));
         if (pot) memcpy(pot + lo, h_out_ + L.pot + 8 * lo, 8 * (hi - lo));
