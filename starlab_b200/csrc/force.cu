@@ -691,7 +691,17 @@ __device__ __forceinline__ void process_task(const ForceParams &p, int itile_idx
                 const int i = ib + k;
                 if (i >= p.ni) continue;
                 Partial a = load_partial_cg(p.part + i);
-                for (int sp = 1; sp < p.nsplit; ++sp) add_partial(a, load_partial_cg(p.part + (size_t)sp * p.ni + i));
+                // Split order kept; four loads in flight per step (the fold is
+                // latency-bound when there are many splits).
+                int sp = 1;
+                for (; sp + 4 <= p.nsplit; sp += 4) {
+                    Partial b[4];
+#pragma unroll
+                    for (int u = 0; u < 4; ++u) b[u] = load_partial_cg(p.part + (size_t)(sp + u) * p.ni + i);
+#pragma unroll
+                    for (int u = 0; u < 4; ++u) add_partial(a, b[u]);
+                }
+                for (; sp < p.nsplit; ++sp) add_partial(a, load_partial_cg(p.part + (size_t)sp * p.ni + i));
                 write_final(p, i, a);
             }
             if (threadIdx.x == 0) p.tile_counter[itile_idx] = 0;
@@ -849,10 +859,14 @@ ForceConfig choose_config(int kmode, int ni, int nj_pad, int num_sms, bool nb) {
     // paired layout already reuses each loaded j-pair twice and runs out of
     // registers at 2 (measured: 91 ms vs 95 ms for the N = 262144 sweep).
     c.r = ((kmode == kKernMixedDS || kmode == kKernF64) && c.il == 32 && ni >= 8192) ? 2 : 1;
-    // i-groups per CTA: as many warps on distinct i as there are i's.
+    // i-groups per CTA: at most an eighth of the i-block per CTA, so that a
+    // mid-size block spreads over several i-tiles instead of one i-tile
+    // split many ways -- whose split fold (one thread per i over all splits)
+    // then dominates.  Measured at nj = 262144 (mixed): ni = 256 0.12 vs
+    // 0.31 ms, ni = 1024 0.39 vs 0.43 ms; ni >= 2048 unchanged (8 groups).
     int groups_needed = (ni + c.il * c.r - 1) / (c.il * c.r);
     int G = 1;
-    while (G * 2 <= c.warps && G * 2 <= groups_needed) G *= 2;
+    while (G * 2 <= c.warps && G * 2 * 8 <= groups_needed) G *= 2;
     c.H = c.warps / G;
     const int T = tile_size(kmode);
     const int JL = 32 / c.il;
@@ -862,8 +876,10 @@ ForceConfig choose_config(int kmode, int ni, int nj_pad, int num_sms, bool nb) {
     const int itile = G * c.il * c.r;
     const int n_itiles = (ni + itile - 1) / itile;
     const int ntiles = nj_pad / T;
-    // Fill the GPU with whole waves: 2 resident CTAs per SM.
-    const int slots = 2 * num_sms;
+    // Fill the GPU with whole waves: 2 resident CTAs per SM, or one per SM
+    // for blocks of up to 128 i (fewer splits to fold: ni = 64 0.051 vs
+    // 0.062 ms, ni = 16 0.042 vs 0.058 ms).
+    const int slots = (ni <= 128 ? 1 : 2) * num_sms;
     int best_split = 1;
     double best_eff = -1;
     for (int sp = 1; sp <= ntiles && sp <= 4096; ++sp) {
