@@ -83,7 +83,10 @@ def test_concurrent_clients():
     for t in th:
         t.join(timeout=120)
     assert len(results) == nclients
-    # every call equals the plain engine's answer for the same inputs
+    # every call equals the plain engine's answer for the same inputs, to
+    # the mixed mode's rounding: the batched launch and a single call
+    # partition the j-range over threads differently, so their FP32 chunk
+    # sums round differently (nn, from the same pair r^2, stays exact)
     for k in range(nclients):
         c, (m, x, v, a, j) = data[k]
         eng = G6Engine(cluster_id=5000 + k, precision="mixed", npipes=len(m))
@@ -91,7 +94,7 @@ def test_concurrent_clients():
         eng.set_ti(0.0)
         for idx, got in results[k]:
             want = eng.force(len(m), idx, x[idx], v[idx], EPS2)
-            assert rel_err_vec(got[0], want[0]).max() < 1e-9
+            assert rel_err_vec(got[0], want[0]).max() < 1e-6
             assert np.array_equal(got[3], want[3])
         eng.close()
     srv.close()
