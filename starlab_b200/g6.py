@@ -198,8 +198,11 @@ class G6Engine:
         ni = index.shape[0]
         xi, vi = _vec(xi, ni), _vec(vi, ni)
         hh = None if h2 is None else np.ascontiguousarray(np.broadcast_to(np.asarray(h2, np.float64), (ni,)))
-        zeros3 = np.zeros((max(ni, 1), 3))
-        zeros1 = np.zeros(max(ni, 1))
+        # aold/j6old/phiold are scaling hints the engine does not use: one
+        # zero buffer, kept between calls
+        if getattr(self, "_zeros3", None) is None or self._zeros3.shape[0] < max(ni, 1):
+            self._zeros3, self._zeros1 = np.zeros((max(ni, 1), 3)), np.zeros(max(ni, 1))
+        zeros3, zeros1 = self._zeros3, self._zeros1
         self._keep = (index, xi, vi, hh)
         c_nj, c_ni, c_e = ctypes.c_int(int(nj)), ctypes.c_int(ni), ctypes.c_double(eps2)
         self.lib.g6calc_firsthalf_(ctypes.byref(self._cid), ctypes.byref(c_nj), ctypes.byref(c_ni),
@@ -210,13 +213,15 @@ class G6Engine:
                                    ctypes.byref(c_e), _ptr(hh))
         self._pending = (int(nj), ni, float(eps2))
 
-    def calc_lasthalf2(self, ni=None):
+    def calc_lasthalf2(self, ni=None, out=None):
+        """g6calc_lasthalf2_; `out` = (acc, jerk, pot, nn) C-contiguous arrays
+        to write into (else new ones are returned)."""
         nj, n, eps2 = self._pending
         ni = n if ni is None else ni
-        acc = np.empty((ni, 3))
-        jerk = np.empty((ni, 3))
-        pot = np.empty(ni)
-        nn = np.empty(ni, dtype=np.int32)
+        if out is None:
+            acc, jerk, pot, nn = np.empty((ni, 3)), np.empty((ni, 3)), np.empty(ni), np.empty(ni, dtype=np.int32)
+        else:
+            acc, jerk, pot, nn = out
         index, xi, vi, hh = self._keep
         c_nj, c_ni, c_e = ctypes.c_int(nj), ctypes.c_int(ni), ctypes.c_double(eps2)
         rc = self.lib.g6calc_lasthalf2_(ctypes.byref(self._cid), ctypes.byref(c_nj), ctypes.byref(c_ni),
@@ -252,9 +257,7 @@ class G6Engine:
             e = min(ni, s + npipes)
             hh = None if h2 is None else np.broadcast_to(np.asarray(h2, np.float64), (ni,))[s:e]
             self.calc_firsthalf(nj, index[s:e], xi[s:e], vi[s:e], eps2, hh)
-            res = self.calc_lasthalf2()
-            for o, r in zip(outs, res):
-                o[s:e] = r
+            self.calc_lasthalf2(out=tuple(o[s:e] for o in outs))
         return tuple(outs)
 
     def sweep(self, nj, i0=0, ni=None, eps2=0.0, copy_out=True):
