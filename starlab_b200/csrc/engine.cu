@@ -374,7 +374,6 @@ int Engine::set_j_bulk(int n, const int *address, const int *index, const double
     Part parts[9];
     int np = 0;
     size_t off = 0;
-    const void *dev[9];
     auto add = [&](const void *src, size_t b) -> const void * {
         if (!src) return nullptr;
         parts[np++] = {src, b, off};
@@ -392,7 +391,6 @@ int Engine::set_j_bulk(int n, const int *address, const int *index, const double
     b.k18 = static_cast<const double *>(add(k18, vec));
     b.addr = static_cast<const int *>(add(address, 4 * nd));
     b.index = static_cast<const int *>(add(index, 4 * nd));
-    (void)dev;
     double tmax[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     parallel_ranges(nd, 16384, [&](size_t lo, size_t hi, size_t t) {
         for (int k = 0; k < np; ++k) {
