@@ -344,7 +344,7 @@ int Engine::set_j_bulk(int n, const int *address, const int *index, const double
     if (flush_j()) return -1;  // earlier single updates land first
     G6_CHECK(cudaSetDevice(device_), "cudaSetDevice");
     const size_t nd = (size_t)n, vec = 24 * nd;
-    const size_t bytes = 16 * nd + 5 * vec + 8 * nd + 64;
+    const size_t bytes = 16 * nd + 5 * vec + 8 * nd + 9 * 16;  // nine arrays, each start 16-byte aligned
     if (bytes > bulk_cap_) {
         G6_CHECK(cudaStreamSynchronize(stream_), "sync");
         if (d_bulk_) cudaFree(d_bulk_);

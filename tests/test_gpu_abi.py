@@ -120,8 +120,9 @@ def test_bulk_upload_equals_single_updates(oracle):
     permuted addresses, index != address, a repeated address (last write
     wins, as n single g6_set_j_particle_ calls), and single updates before
     and after, must leave exactly the j-memory the single calls leave."""
-    n = 6000
+    n = 6001  # odd: every one of the nine gathered arrays ends off the 16-byte grid
     m, x, v, a, j = snapshot(n, 21)
+    k18 = np.random.default_rng(5).normal(size=(n, 3)) * 1e-3
     rng = np.random.default_rng(4)
     perm = rng.permutation(n).astype(np.int32)
     index = perm.copy()
@@ -132,9 +133,9 @@ def test_bulk_upload_equals_single_updates(oracle):
     e1, e2 = eng(), eng()
     # a single update staged before the bulk upload, overwritten by it
     e1.set_j_particle(int(perm[5]), 0.0, 9.0, z, z, z, z, np.ones(3))
-    e1.set_j_particles(0.0, m, j / 6.0, 0.5 * a, v, x, address=perm, index=index)
+    e1.set_j_particles(0.0, m, j / 6.0, 0.5 * a, v, x, k18=k18, address=perm, index=index)
     e1.set_j_particles(0.0, m[:10], (j / 6.0)[:10], (0.5 * a)[:10], v[:10], x[:10] * 1.01, address=perm[:10])
-    e1.set_j_particles(0.0, m, j / 6.0, 0.5 * a, v, x, address=dup_addr, index=index)
+    e1.set_j_particles(0.0, m, j / 6.0, 0.5 * a, v, x, k18=k18, address=dup_addr, index=index)
     e1.set_j_particle(int(perm[7]), 0.0, m[7], z, (j / 6.0)[7], (0.5 * a)[7], v[7], x[7] * 0.99)
     for k in range(n):
         e2.set_j_particle(int(perm[k]), 0.0, m[k], z, (j / 6.0)[k], (0.5 * a)[k], v[k], x[k], index=int(index[k]))
