@@ -247,7 +247,10 @@ void g6b200_ens_destroy(g6b200_ensemble *h);
  * stream, so short calls are not held behind long ones; calls arriving while
  * a launch runs join the next one.  Every call predicts its cluster's
  * j-set into its own buffer, so calls of one cluster at different block times
- * may share a launch.  A call's results do not depend on which other calls
+ * may share a launch.  A call sees the j-particles loaded before its launch is
+ * dispatched, so a client that updates j-particles between calls (as kira
+ * does after each block) waits for a call before loading the next updates.
+ * A call's results do not depend on which other calls
  * share its launch (bit-identical alone or mixed).  precision: G6B200_FP64 or
  * G6B200_MIXED.  No neighbour lists on this path. */
 typedef struct g6b200_server g6b200_server;

@@ -636,6 +636,10 @@ int Ensemble::push_host_state() {
     return 0;
 }
 
+// Kernels launched by one iteration: schedule, scan, predict, force, and
+// (mode != 2) the corrector.
+constexpr int kLaunchesPerIteration = 5;
+
 int Ensemble::iteration(int mode) {
     ens_schedule_kernel<<<nc_, kSchedThreads, 0, stream_>>>(d_, mode);
     ens_scan_kernel<<<1, 1024, 0, stream_>>>(d_);
@@ -679,6 +683,16 @@ int Ensemble::run_batched(double t_end, EnsembleStats *st, int tune) {
     ECHK(cudaStreamSynchronize(stream_), "cap");
     auto t0 = std::chrono::steady_clock::now();
     long long iters = 0;
+    // Events and the pinned flag word are released on every return.
+    struct Scratch {
+        cudaEvent_t e0 = nullptr, e1 = nullptr;
+        int *h_active = nullptr;
+        ~Scratch() {
+            if (e0) cudaEventDestroy(e0);
+            if (e1) cudaEventDestroy(e1);
+            if (h_active) cudaFreeHost(h_active);
+        }
+    } sc;
     // Autotune the launch shape on the first iterations of the run: the
     // i-tile of large blocks (H warps per j-tile: i per CTA = 256 / H) and
     // the j-split factor (tasks wanted per cluster), by measured time per
@@ -688,9 +702,9 @@ int Ensemble::run_batched(double t_end, EnsembleStats *st, int tune) {
         const int targets[3] = {296, 592, 1184};
         double best = 1e30;
         int bestH = d_.cfg.H, bestT = d_.cfg.nsplit;
-        cudaEvent_t e0, e1;
-        cudaEventCreate(&e0);
-        cudaEventCreate(&e1);
+        ECHK(cudaEventCreate(&sc.e0), "event");
+        ECHK(cudaEventCreate(&sc.e1), "event");
+        cudaEvent_t e0 = sc.e0, e1 = sc.e1;
         for (int tt : targets) {
             for (int h : hs) {
                 d_.cfg.H = h;
@@ -711,8 +725,6 @@ int Ensemble::run_batched(double t_end, EnsembleStats *st, int tune) {
                 }
             }
         }
-        cudaEventDestroy(e0);
-        cudaEventDestroy(e1);
         d_.cfg.H = bestH;
         d_.cfg.nsplit = bestT;
         ctas_ = batch_ctas(kmode_, d_.cfg, num_sms_);
@@ -729,12 +741,10 @@ int Ensemble::run_batched(double t_end, EnsembleStats *st, int tune) {
     ECHK(cudaStreamEndCapture(stream_, &g), "capture");
     ECHK(cudaGraphInstantiate(&graph_, g, 0), "instantiate");
     cudaGraphDestroy(g);
-    int *h_active = nullptr;
-    ECHK(cudaMallocHost(&h_active, sizeof(int)), "pinned");
-    long long launches = 0;
+    ECHK(cudaMallocHost(&sc.h_active, sizeof(int)), "pinned");
+    int *h_active = sc.h_active;
     for (;;) {
         ECHK(cudaGraphLaunch(graph_, stream_), "graph launch");
-        launches += K * 6;
         iters += K;
         cudaMemcpyAsync(h_active, d_.active, sizeof(int), cudaMemcpyDeviceToHost, stream_);
         ECHK(cudaStreamSynchronize(stream_), "run");
@@ -742,11 +752,9 @@ int Ensemble::run_batched(double t_end, EnsembleStats *st, int tune) {
         if (iters > max_iters_ ||
             std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count() > max_seconds_) {
             err = "ensemble: iteration or time limit reached";
-            cudaFreeHost(h_active);
             return -1;
         }
     }
-    cudaFreeHost(h_active);
     auto t1 = std::chrono::steady_clock::now();
     unsigned long long i1 = 0;
     unsigned status = 0;
@@ -760,7 +768,7 @@ int Ensemble::run_batched(double t_end, EnsembleStats *st, int tune) {
         st->seconds = std::chrono::duration<double>(t1 - t0).count();
         st->interactions = (long long)(i1 - i0);
         st->iterations = iters;
-        st->launches = launches;
+        st->launches = iters * kLaunchesPerIteration;
     }
     return 0;
 }

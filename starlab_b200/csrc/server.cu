@@ -4,13 +4,14 @@
 // cluster) submit force calls -- a block time, an i-block and its predicted
 // positions/velocities, exactly the content of one g6calc_firsthalf_ -- and
 // later wait for the results (g6calc_lasthalf2_'s outputs).  A dispatcher
-// thread takes every pending call (at most one per cluster at a time, since a
-// cluster's calls are sequential), prepares each cluster's j-memory (staged
-// updates, prediction to the call's block time) on that cluster's stream, and
-// runs all calls as ONE persistent launch over their (call, i-tile, j-split)
-// work list.  Calls that arrive while a batch is on the GPU join the next
-// one.  Each call's split plan depends on its own sizes only, so its results
-// are bit-identical alone and in any mix.
+// thread takes every pending call of its lane, prepares each call's j-set
+// (the cluster's staged updates, then a prediction to the call's block time
+// into a buffer of the call's own, so two calls of one cluster may share a
+// batch) on that cluster's stream, and runs all calls as ONE launch over
+// their (call, i-tile, j-split) work list.  A call sees the j-particles
+// loaded before its batch is dispatched.  Calls that arrive while a batch is
+// on the GPU join the next one.  Each call's split plan depends on its own
+// sizes only, so its results are bit-identical alone and in any mix.
 //
 // Cluster j-state stays resident on the device.  Admission: opening a
 // cluster reserves its HBM footprint against a budget; when the budget is
