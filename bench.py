@@ -31,6 +31,11 @@ Reported (one JSON line on rank 0):
                N = 65536 Plummer sphere through h3calc_ in h3npipe_() chunks,
                the block stored at the block time as kira's GRAPE-4 branch
                does; wall-clock interactions/s through the ABI
+  story        story-format snapshot input: a 262144-body snapshot in the
+               reference's own output format read by the GPU reader
+               (include/g6b200_story.h), text resident on the device and from
+               host bytes; the reference's get_dyn on the same text as the
+               CPU baseline
 
 Multi-GPU (torchrun, one rank per GPU): every rank integrates its own
 independent cluster (different seed) -- weak scaling, no collective on the
@@ -71,6 +76,7 @@ def parse():
     ap.add_argument("--ensemble-clusters", type=int, default=256)
     ap.add_argument("--ensemble-t", type=float, default=1.0)
     ap.add_argument("--no-grape4", action="store_true")
+    ap.add_argument("--no-story", action="store_true")
     return ap.parse_args()
 
 
@@ -251,6 +257,57 @@ def grape4_section(seed, n=65536, sweeps=3):
             "interactions_per_s": inter / sec, "calls_per_sweep": (s1["calls"] - s0["calls"]) // sweeps,
             "launches_per_sweep": (s1["launches"] - s0["launches"]) // sweeps,
             "path": "h3mjpdma_indirect_/h3calc_ (host buffers, wall clock)"}
+
+
+def story_section(seed, n=262144, reps=10, cpu=True):
+    """Story-format snapshot input: a flat n-body snapshot (root + n leaves,
+    "%.18g" numbers as the reference's put_node writes them) read through the
+    reader's C ABI; the reference's own get_dyn on the same text as the CPU
+    baseline (oracle/_ref/story_ref, one core)."""
+    import torch
+    from starlab_b200 import ics
+    from starlab_b200.story import StoryReader, format_story
+    m = ics.salpeter_masses(n, seed)
+    _, x, v = ics.plummer(n, seed + 1, masses=m)
+    text = format_story(m, x + 1e-3, v - 5e-4, log_lines=[" ===>  bench snapshot"])
+    rd = StoryReader()
+    d = torch.frombuffer(bytearray(text), dtype=torch.uint8).cuda()
+    out = {"n": n, "bytes": len(text), "workload": "flat snapshot, root + %d leaves, Plummer/Salpeter" % n}
+    for raw in (False, True):
+        for _ in range(3):
+            rd.parse_device(d.data_ptr(), d.numel(), raw=raw)
+        ts = []
+        for _ in range(reps):
+            t0 = time.perf_counter()
+            info = rd.parse_device(d.data_ptr(), d.numel(), raw=raw)
+            ts.append(time.perf_counter() - t0)
+        sec = statistics.median(ts)
+        out["device_raw" if raw else "device"] = {"ms": sec * 1e3, "particles_per_s": n / sec,
+                                                 "text_gbs": len(text) / sec / 1e9}
+    ts = []
+    for _ in range(max(3, reps // 2)):
+        t0 = time.perf_counter()
+        info = rd.parse_info(text)
+        lm, lx, lv = rd.leaves(info)
+        ts.append(time.perf_counter() - t0)
+    sec = statistics.median(ts)
+    out["e2e"] = {"ms": sec * 1e3, "particles_per_s": n / sec, "h2d_bytes": len(text), "d2h_bytes": 56 * n,
+                  "path": "g6b200_story_parse (host bytes) + g6b200_story_leaves"}
+    if cpu:
+        from oracle.oracle import STORY_REF, StoryOracle, ref_story_seconds
+        o = StoryOracle().parse(text)
+        out["matches_oracle"] = bool(np.array_equal(o.leaves_pos.view(np.uint64), lx.view(np.uint64)) and
+                                     np.array_equal(o.leaves_vel.view(np.uint64), lv.view(np.uint64)) and
+                                     np.array_equal(o.leaves_mass.view(np.uint64), lm.view(np.uint64)))
+        if os.path.exists(STORY_REF):
+            with tempfile.NamedTemporaryFile(suffix=".snap") as f:
+                f.write(text)
+                f.flush()
+                secs = ref_story_seconds(f.name)
+            out["cpu_baseline"] = {"value": n / secs, "unit": "particles/s", "cores": 1, "kind": "reference",
+                                   "seconds": secs, "sample": "the same snapshot read by get_dyn"}
+    rd.close()
+    return out
 
 
 def _rel(a, b):
@@ -473,6 +530,8 @@ def main():
             line["served_stream"] = served_section(5)
         if dist.world == 1 and not args.no_grape4:
             line["grape4"] = grape4_section(7)
+        if dist.world == 1 and not args.no_story:
+            line["story"] = story_section(11, cpu=not args.no_cpu_baseline)
         if dist.world == 1 and not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(n, seed, os.cpu_count() or 1, gpu=(acc, jerk, pot, nn))
         print(json.dumps(line), flush=True)

@@ -18,6 +18,9 @@ with g++ directly (no autotools: they are absent here), into ``oracle/_ref/``:
                        ``libg6b200.so`` before the stubs, i.e. the unchanged
                        caller driving the GPU engine through the g6 ABI
                        (built only when the engine library exists);
+* ``story_ref``         ``oracle/story_ref.C``: the reference's snapshot
+                       reader (``get_dyn``) run on a story text, every node
+                       printed exactly (hex floats), or ``-t``: its time;
 * ``libref_force.so``  ``oracle/ref_force.C``: a C entry point over the
                        reference's ``predict_loworder`` and
                        ``hdyn::flat_calculate_acc_and_jerk``
@@ -166,6 +169,8 @@ def main():
         tool_objs[name] = obj
     harness_obj = os.path.join(OUT, "obj", "ref_force.o")
     add(os.path.join(HERE, "ref_force.C"), harness_obj)
+    story_obj = os.path.join(OUT, "obj", "story_ref.o")
+    add(os.path.join(HERE, "story_ref.C"), story_obj)
     g4_obj = os.path.join(OUT, "obj", "hdyn_grape4_half_chip.o")
     add(os.path.join(src, "node/dyn/hdyn/evolve/hdyn_grape4.C"), g4_obj, extra=["-DUSE_HALF_CHIP=1"])
     oobj = {}
@@ -200,6 +205,9 @@ def main():
         exe = os.path.join(OUT, name)
         if not up_to_date(exe, [obj, lib, stubs]):
             run(["g++", "-o", exe, obj, lib, stubs] + link_tail)
+    exe = os.path.join(OUT, "story_ref")
+    if not up_to_date(exe, [story_obj, lib, stubs]):
+        run(["g++", "-o", exe, story_obj, lib, stubs] + link_tail)
     so = os.path.join(OUT, "libref_force.so")
     if not up_to_date(so, [harness_obj, lib, stubs]):
         run(["g++", "-shared", "-o", so, harness_obj, "-Wl,--whole-archive", lib,

@@ -9,6 +9,10 @@
   the GRAPE-4 pipeline (oracle/g4_oracle.c).
 * ``Harp3Sim``  -- oracle/_ref/libharp3sim.so, the reference's own IEEE
   GRAPE-4 simulator (src/harpsims/harp3fastsim.c) driven through its ABI.
+* ``StoryOracle`` -- oracle/_build/libstoryoracle.so, the sequential C
+  restatement of the reference's snapshot reader (oracle/story_oracle.c).
+* ``ref_story`` -- oracle/_ref/story_ref, the reference's own get_dyn run on
+  a text, every value printed exactly.
 """
 import ctypes
 import os
@@ -20,6 +24,8 @@ ORACLE_LIB = os.path.join(HERE, "_build", "libg6oracle.so")
 REF_LIB = os.path.join(HERE, "_ref", "libref_force.so")
 G4_ORACLE_LIB = os.path.join(HERE, "_build", "libg4oracle.so")
 HARP3_LIB = os.path.join(HERE, "_ref", "libharp3sim.so")
+STORY_ORACLE_LIB = os.path.join(HERE, "_build", "libstoryoracle.so")
+STORY_REF = os.path.join(HERE, "_ref", "story_ref")
 
 _P = ctypes.c_void_p
 
@@ -198,3 +204,113 @@ class Harp3Sim:
                 got = self.lib.h3nblist_(self._i(0), self._i(c), _p(buf))
                 lists.append(buf[:got].copy())
         return acc, jerk, lists
+
+
+class StorySnapshot:
+    """Flat arrays of a parse (same names as starlab_b200.story.Snapshot)."""
+
+
+def leaves_relative_to_root(parent, pos, vel):
+    """Leaves (nodes without daughters, roots excluded) in pre-order, with
+    positions/velocities summed from the leaf up to the root (excluded),
+    starting at +0 -- something_relative_to_root, dyn_tt.C:94-110."""
+    n = parent.size
+    has_d = np.zeros(n, bool)
+    has_d[parent[parent >= 0]] = True
+    leaves = np.flatnonzero((~has_d) & (parent >= 0)).astype(np.int32)
+    x = np.zeros((leaves.size, 3))
+    v = np.zeros((leaves.size, 3))
+    cur = leaves.copy()
+    while True:
+        act = parent[cur] >= 0
+        if not act.any():
+            break
+        x[act] = x[act] + pos[cur[act]]
+        v[act] = v[act] + vel[cur[act]]
+        cur = np.where(act, parent[cur], cur)
+    return leaves, x, v
+
+
+class StoryOracle:
+    """The C restatement of get_dyn over a whole text."""
+
+    def __init__(self, path=STORY_ORACLE_LIB):
+        if not os.path.exists(path):
+            raise ImportError("story oracle library missing: %s" % path)
+        self.lib = ctypes.CDLL(path)
+        LLP = ctypes.POINTER(ctypes.c_longlong)
+        self.lib.so_parse.restype = ctypes.c_void_p
+        self.lib.so_parse.argtypes = [ctypes.c_char_p, ctypes.c_longlong, ctypes.c_int, LLP, LLP, LLP,
+                                      ctypes.POINTER(ctypes.c_char_p)]
+        self.lib.so_error.argtypes = [ctypes.c_void_p]
+        self.lib.so_get.argtypes = [ctypes.c_void_p] + [ctypes.c_void_p] * 9
+        self.lib.so_free.argtypes = [ctypes.c_void_p]
+
+    def parse(self, text, raw=False):
+        """A StorySnapshot, or raises ValueError(line, what) on an error."""
+        nn, nr, el = ctypes.c_longlong(), ctypes.c_longlong(), ctypes.c_longlong()
+        what = ctypes.c_char_p()
+        h = self.lib.so_parse(text, len(text), 1 if raw else 0, ctypes.byref(nn), ctypes.byref(nr), ctypes.byref(el),
+                              ctypes.byref(what))
+        try:
+            if self.lib.so_error(h):
+                raise ValueError(int(el.value), what.value.decode() if what.value else "")
+            n, r = nn.value, nr.value
+            s = StorySnapshot()
+            s.parent, s.index = np.empty(n, np.int32), np.empty(n, np.int32)
+            s.name_offset, s.name_length = np.empty(n, np.int32), np.empty(n, np.int32)
+            s.mass, s.pos, s.vel = np.empty(n), np.empty((n, 3)), np.empty((n, 3))
+            s.root_node, s.system_time = np.empty(r, np.int32), np.empty(r)
+            self.lib.so_get(h, _p(s.parent), _p(s.index), _p(s.name_offset), _p(s.name_length), _p(s.mass),
+                            _p(s.pos), _p(s.vel), _p(s.root_node), _p(s.system_time))
+        finally:
+            self.lib.so_free(h)
+        s.leaves_node, s.leaves_pos, s.leaves_vel = leaves_relative_to_root(s.parent, s.pos, s.vel)
+        s.leaves_mass = s.mass[s.leaves_node]
+        s.leaves_index = s.index[s.leaves_node]
+        return s
+
+
+def ref_story(text, path=STORY_REF, timeout=600):
+    """Run the reference's get_dyn on text (oracle/_ref/story_ref): a
+    StorySnapshot with names as strings, or None if the harness is not
+    built.  A reference exit shows as RuntimeError."""
+    import subprocess
+    if not os.path.exists(path):
+        return None
+    r = subprocess.run([path], input=text, stdout=subprocess.PIPE, stderr=subprocess.PIPE, timeout=timeout)
+    if r.returncode != 0:
+        raise RuntimeError("reference reader exited %d: %s" % (r.returncode, r.stderr[-500:].decode("latin-1")))
+    parent, index, names, vals, lv, times = [], [], [], [], [], []
+    for line in r.stdout.decode("latin-1").splitlines():
+        f = line.split(" ")
+        if f[0] == "P":
+            parent.append(int(f[1]))
+            index.append(int(f[2]))
+            ln, _, nm = f[3].partition(":")
+            names.append(None if int(ln) < 0 else nm)
+            vals.append([float.fromhex(x) for x in f[4:11]])
+        elif f[0] == "L":
+            lv.append([float.fromhex(x) for x in f[1:7]])
+        elif f[0] == "T":
+            times.append(float.fromhex(f[1]))
+    s = StorySnapshot()
+    s.parent = np.array(parent, np.int32)
+    s.index = np.array(index, np.int32)
+    s.names = names
+    v = np.array(vals, np.float64).reshape(-1, 7)
+    s.mass, s.pos, s.vel = v[:, 0].copy(), v[:, 1:4].copy(), v[:, 4:7].copy()
+    l6 = np.array(lv, np.float64).reshape(-1, 6)
+    s.leaves_pos, s.leaves_vel = l6[:, :3].copy(), l6[:, 3:].copy()
+    s.system_time = np.array(times)
+    return s
+
+
+def ref_story_seconds(path_to_text, path=STORY_REF, timeout=900):
+    """Seconds the reference's get_dyn loop takes on a file (story_ref -t)."""
+    import subprocess
+    with open(path_to_text, "rb") as f:
+        r = subprocess.run([path, "-t"], stdin=f, stdout=subprocess.PIPE, stderr=subprocess.PIPE, timeout=timeout)
+    if r.returncode != 0:
+        raise RuntimeError("reference reader exited %d" % r.returncode)
+    return float(r.stdout.split()[1])

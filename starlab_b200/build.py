@@ -6,9 +6,10 @@
 * ``starlab_b200/lib/libh3b200.so`` -- the GRAPE-4 ABI of ``include/h3b200.h``:
   ``grape4.cu`` with the engine objects it drives (a library of its own, since
   kira takes its GRAPE-4 branch whenever ``h3npipe_()`` answers).
-* ``oracle/_build/libg6oracle.so`` / ``libg4oracle.so`` -- the oracle's C
-  restatements ``oracle/g6_oracle.c`` and ``oracle/g4_oracle.c`` (test
-  infrastructure) with gcc, FP contraction off.
+* ``oracle/_build/libg6oracle.so`` / ``libg4oracle.so`` / ``libstoryoracle.so``
+  -- the oracle's C restatements ``oracle/g6_oracle.c``, ``oracle/g4_oracle.c``
+  and ``oracle/story_oracle.c`` (test infrastructure) with gcc, FP
+  contraction off.
 
 Usage: ``python -m starlab_b200.build [--verbose] [--ptxas-v]``.
 """
@@ -31,6 +32,8 @@ ORACLE_SRC = os.path.join(REPO, "oracle", "g6_oracle.c")
 ORACLE_LIB = os.path.join(REPO, "oracle", "_build", "libg6oracle.so")
 ORACLE_G4_SRC = os.path.join(REPO, "oracle", "g4_oracle.c")
 ORACLE_G4_LIB = os.path.join(REPO, "oracle", "_build", "libg4oracle.so")
+ORACLE_STORY_SRC = os.path.join(REPO, "oracle", "story_oracle.c")
+ORACLE_STORY_LIB = os.path.join(REPO, "oracle", "_build", "libstoryoracle.so")
 
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -63,6 +66,7 @@ def build_engine(verbose=False, ptxas_v=False, force=False):
     headers = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".h", ".cuh"))]
     headers.append(os.path.join(REPO, "include", "g6b200.h"))
     headers.append(os.path.join(REPO, "include", "h3b200.h"))
+    headers.append(os.path.join(REPO, "include", "g6b200_story.h"))
     objs, jobs = [], []
     for f in srcs:
         src = os.path.join(CSRC, f)
@@ -87,7 +91,7 @@ def build_engine(verbose=False, ptxas_v=False, force=False):
 
 def build_oracle(verbose=False):
     os.makedirs(os.path.dirname(ORACLE_LIB), exist_ok=True)
-    for src, lib in ((ORACLE_SRC, ORACLE_LIB), (ORACLE_G4_SRC, ORACLE_G4_LIB)):
+    for src, lib in ((ORACLE_SRC, ORACLE_LIB), (ORACLE_G4_SRC, ORACLE_G4_LIB), (ORACLE_STORY_SRC, ORACLE_STORY_LIB)):
         if not _newer(lib, [src]):
             _run(["gcc", "-O2", "-fPIC", "-shared", "-ffp-contract=off", "-o", lib, src, "-lm"], verbose)
     return ORACLE_LIB

@@ -1,0 +1,123 @@
+"""Story-format test texts for the snapshot reader (shared by the CPU and GPU
+tests and the golden-fixture script).
+
+* ``flat_text``         -- a root and n leaves, as put_node writes one
+  (starlab_b200.story.format_story), Salpeter masses, centre of mass off the
+  origin so that check_and_correct_node moves every leaf;
+* ``hierarchy_text``    -- several snapshots of nested binaries and triples
+  with Log stories holding chapters, Star/Hydro sections, extra Dynamics keys
+  the dyn reader keeps as story text, names, repeated keys (the last wins),
+  missing fields (defaults), root system times, and numbers in every form
+  strtod reads (exponents, signs, integers, short and long mantissas);
+* ``MALFORMED``         -- texts the reference cannot read (it exits or reads
+  past its buffer) or that this reader rejects; each must give an error.
+"""
+import numpy as np
+
+from starlab_b200.ics import plummer, salpeter_masses
+from starlab_b200.story import format_story
+
+
+def flat_text(n, seed, shift=(1e-3, -2e-3, 5e-4)):
+    m = salpeter_masses(n, seed)
+    _, x, v = plummer(n, seed + 1, masses=m)
+    x = x + np.asarray(shift)
+    v = v - 0.5 * np.asarray(shift)
+    return format_story(m, x, v, system_time=0.0,
+                        log_lines=[" ===>  synthetic snapshot", "       seed = %d" % seed, "  initial_mass = 1"])
+
+
+def _num(rng, x):
+    r = rng.random()
+    if r < 0.55:
+        return "%.18g" % x
+    if r < 0.7:
+        return "%.17g" % x
+    if r < 0.8:
+        return "%.6e" % x
+    if r < 0.88:
+        return "%+.10g" % x
+    if r < 0.94:
+        return "%.25g" % x
+    return "%.3f" % x
+
+
+def _node(rng, out, depth, idx, names):
+    out.append("(Particle")
+    if rng.random() < 0.9:
+        out.append("  i = %d" % idx[0])
+    if rng.random() < 0.15:
+        nm = "b%d_%d" % (depth, idx[0])
+        names.append(nm)
+        out.append("  name = %s" % nm)
+    idx[0] += 1
+    n_d = 0
+    if depth < 4 and rng.random() < (0.6 if depth == 0 else 0.25):
+        n_d = 2 if rng.random() < 0.8 else 3
+    out.append("  N = %d" % max(n_d, 1))
+    out.append("(Log")
+    if rng.random() < 0.3:
+        out += ["  note = log line", "(Chapter one", "  inner = 1", "(sub", "  deeper", ")sub", ")Chapter one"]
+    out.append(")Log")
+    out.append("(Dynamics")
+    m = float(rng.uniform(0.1, 2.0))
+    x = rng.normal(size=3) * 10.0 ** rng.integers(-6, 2)
+    v = rng.normal(size=3)
+    if rng.random() < 0.9:
+        out.append("  m  =  " + _num(rng, m))
+    if rng.random() < 0.9:
+        out.append("  r  =  " + " ".join(_num(rng, c) for c in x))
+    if rng.random() < 0.9:
+        out.append("  v  =  " + " ".join(_num(rng, c) for c in v))
+    if rng.random() < 0.3:
+        out.append("  a  =  1 2 3")
+        out.append("  pot  =  -0.5")
+        out.append("  t  =  0.125")
+    if rng.random() < 0.1:
+        out.append("  m  =  " + _num(rng, m * 1.5))     # a repeated key: the last one wins
+    if rng.random() < 0.05:
+        out.append("  r  =  1e-3 -2E+1 +7")
+    out.append(")Dynamics")
+    out += ["(Hydro", ")Hydro", "(Star"]
+    if depth == 0:
+        out += ["  mass_scale     =  -1", "  size_scale     =  -1", "  time_scale     =  -1"]
+    out.append(")Star")
+    for _ in range(n_d):
+        _node(rng, out, depth + 1, idx, names)
+    out.append(")Particle")
+
+
+def hierarchy_text(seed, roots=3, leaves_per_root=40):
+    rng = np.random.default_rng(seed)
+    out = []
+    idx = [1]
+    names = []
+    for r in range(roots):
+        out += ["(Particle", "  N = %d" % leaves_per_root, "(Log", " ===>  hierarchy %d" % r, ")Log", "(Dynamics"]
+        if r == 1:
+            out.append("  real_system_time  =  0.5")
+        if r != 2:
+            out.append("  system_time  =  " + _num(rng, 0.25 * (r + 1)))
+        out += ["  m  =  1", "  r  =  0 0 0", "  v  =  0 0 0", ")Dynamics", "(Hydro", ")Hydro", "(Star",
+                ")Star"]
+        for _ in range(leaves_per_root):
+            _node(rng, out, 1, idx, names)
+        out.append(")Particle")
+    return ("\n".join(out) + "\n").encode()
+
+
+def _flat_small():
+    return flat_text(5, 3).decode()
+
+
+MALFORMED = {
+    "unclosed particle": "(Particle\n  N = 1\n(Dynamics\n  m = 1\n)Dynamics\n",
+    "top-level key line": "(Particle\n)Particle\n  m = 1\n",
+    "unexpected keyword": "(Particle\n  mass = 1\n)Particle\n",
+    "vector with two reals": "(Particle\n(Dynamics\n  r = 1 2\n)Dynamics\n)Particle\n",
+    "log title mismatch": "(Particle\n(Log\n(abc\n)abd\n)Log\n)Particle\n",
+    "empty line in a log": "(Particle\n(Log\n\n)Log\n)Particle\n",
+    "long log line": "(Particle\n(Log\n  " + "x" * 300 + "\n)Log\n)Particle\n",
+    "stray close at top": ")Particle\n",
+    "NUL byte": "(Particle\n  i = 1\x00\n)Particle\n",
+}

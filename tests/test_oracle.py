@@ -17,7 +17,7 @@ import pytest
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 GOLDEN = sorted(p for p in glob.glob(os.path.join(HERE, "golden", "*.npz"))
-                if not os.path.basename(p).startswith("g4_"))
+                if not os.path.basename(p).startswith(("g4_", "story_")))
 
 
 def test_golden_fixtures_present():
