@@ -16,12 +16,15 @@ sys.path.insert(0, REPO)
 sys.path.insert(0, os.path.dirname(HERE))
 
 from oracle.oracle import ref_story  # noqa: E402
-from story_texts import flat_text, hierarchy_text  # noqa: E402
+from story_texts import VARIANTS, flat_text, hierarchy_text  # noqa: E402
 
 CASES = {
     "story_flat_n64": lambda: flat_text(64, 5),
     "story_hierarchy_3roots": lambda: hierarchy_text(11, roots=3, leaves_per_root=12),
 }
+# one fixture per corner-case text
+for _k, _t in sorted(VARIANTS.items()):
+    CASES["story_variant_" + _k.replace(" ", "_").replace("-", "_")] = (lambda t: (lambda: t))(_t)
 
 
 def main():

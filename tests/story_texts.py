@@ -10,7 +10,13 @@ tests and the golden-fixture script).
   missing fields (defaults), root system times, and numbers in every form
   strtod reads (exponents, signs, integers, short and long mantissas);
 * ``MALFORMED``         -- texts the reference cannot read (it exits or reads
-  past its buffer) or that this reader rejects; each must give an error.
+  past its buffer) or that this reader rejects; each must give an error;
+* ``VARIANTS``          -- small valid texts at the corners of the reference
+  reader's rules: a Dynamics section after the children, repeated sections,
+  blank lines, CRLF endings, tabs, chapters holding key lines inside a
+  Dynamics section or a particle body, Particle-like chapters inside Log and
+  Star, deep nesting, parents of zero or negative mass, every strtod /
+  strtol form, lines cut at 254 characters, an unterminated last line.
 """
 import numpy as np
 
@@ -106,10 +112,6 @@ def hierarchy_text(seed, roots=3, leaves_per_root=40):
     return ("\n".join(out) + "\n").encode()
 
 
-def _flat_small():
-    return flat_text(5, 3).decode()
-
-
 MALFORMED = {
     "unclosed particle": "(Particle\n  N = 1\n(Dynamics\n  m = 1\n)Dynamics\n",
     "top-level key line": "(Particle\n)Particle\n  m = 1\n",
@@ -120,4 +122,66 @@ MALFORMED = {
     "long log line": "(Particle\n(Log\n  " + "x" * 300 + "\n)Log\n)Particle\n",
     "stray close at top": ")Particle\n",
     "NUL byte": "(Particle\n  i = 1\x00\n)Particle\n",
+}
+
+
+def _leaf(i, m, r, v, extra=()):
+    return ["(Particle", "  i = %d" % i, "  N = 1", "(Log", ")Log", "(Dynamics", "  m  =  %s" % m,
+            "  r  =  %s" % r, "  v  =  %s" % v] + list(extra) + [")Dynamics", "(Hydro", ")Hydro", "(Star", ")Star",
+                                                                 ")Particle"]
+
+
+def _root(children, head=()):
+    return ["(Particle", "  N = 2", "(Log", ")Log", "(Dynamics", "  system_time  =  0.5", "  m  =  1",
+            "  r  =  0 0 0", "  v  =  0 0 0", ")Dynamics"] + list(head) + children + [")Particle"]
+
+
+def _j(lines, nl="\n"):
+    return (nl.join(lines) + nl).encode()
+
+
+# Valid texts that exercise the corners of the reference reader's rules.
+VARIANTS = {
+    "dynamics after children": _j(["(Particle", "  i = 10"] + _leaf(1, "0.25", "1 0 0", "0 1 0") +
+                                  _leaf(2, "0.75", "-1 0 0", "0 -1 0") +
+                                  ["(Dynamics", "  m  =  3", "  r  =  0.5 0.5 0.5", "  v  =  0 0 1", ")Dynamics",
+                                   ")Particle"]),
+    "two dynamics sections": _j(_root(_leaf(1, "0.5", "1 2 3", "0 0 0") +
+                                      ["(Particle", "(Dynamics", "  m = 2", ")Dynamics", "(Dynamics", "  m = 0.25",
+                                       "  r = 0.125 0 0", ")Dynamics", ")Particle"])),
+    "blank lines inside": _j(["(Particle", "", "  i = 4", "(Dynamics", "", "  m = 0.5", "", ")Dynamics", "",
+                              ")Particle"] + [""] + ["(Particle", ")Particle"]),
+    "crlf endings": _j(_root(_leaf(1, "0.3", "1 -2 3", "0.5 0 0") + _leaf(2, "0.7", "-1 2 -3", "0 0.5 0")), "\r\n"),
+    "tabs": _j(["(Particle", "\ti\t=\t3", "(Dynamics", "\tm\t=\t1.5", "\tr\t=\t1\t2\t3", "\tv =\t-1 -2\t-3",
+                ")Dynamics", ")Particle"]),
+    "chapter inside dynamics": _j(["(Particle", "(Dynamics", "  m = 1", "(extra", "  m = 3", "  r = 1 1 1", ")extra",
+                                   "  v = 2 2 2", ")Dynamics", ")Particle"]),
+    "chapter in a particle body": _j(["(Particle", "(Foo", "  i = 7", "  name = foo7", ")Foo", "(Dynamics", "  m = 1",
+                                      ")Dynamics", ")Particle"]),
+    "particle-like chapters in log and star": _j(["(Particle", "(Log", "(Particle", "  m = 9", ")Particle", ")Log",
+                                                  "(Star", "(Particle", "  m = 9", ")Particle", ")Star",
+                                                  "(Hydro", "  r = 9 9 9", ")Hydro"] +
+                                                 _leaf(5, "2", "0 0 1", "0 0 0") + [")Particle"]),
+    "deep chain": _j(["(Particle"] * 1 + sum([["(Particle", "  i = %d" % k, "(Dynamics", "  m = %g" % (1 + k),
+                                               "  r = %g 0 0" % (0.1 * k), ")Dynamics"] for k in range(12)], []) +
+                     _leaf(99, "0.5", "0 0.25 0", "0 0 0.5") + [")Particle"] * 12 + [")Particle"]),
+    "zero and negative parent mass": _j(_root(["(Particle"] + _leaf(1, "0", "1 0 0", "0 1 0") +
+                                              _leaf(2, "0", "-1 0 0", "0 -1 0") + [")Particle", "(Particle"] +
+                                              _leaf(3, "-1", "1 1 0", "0 0 0") + _leaf(4, "0.5", "0 1 1", "1 0 0") +
+                                              [")Particle"])),
+    "number forms": _j(_root(_leaf(1, "1.", ".5e1 -0 +7", "1e5 -1E-5 3.") +
+                             _leaf(2, "   0.125   junk", "1 2 3 4", "-.5 +.25e+1 0x") +
+                             _leaf(3, "4.9406564584124654e-324", "1e-320 2.2250738585072014e-308 1e300",
+                                   "1.7976931348623157e308 -1e-310 0"))),
+    "index and name forms": _j(_root(["(Particle", "  i = -5", "  name = a(b)c", "(Dynamics", "  m = 1", ")Dynamics",
+                                      ")Particle", "(Particle", "  i = 99999999999", "  name =   spaced  name",
+                                      ")Particle", "(Particle", "  i = +12abc", "  i = 13", ")Particle"])),
+    "cut at 254 characters": _j(["(Particle", "(Dynamics", "  m  =  " + " " * 240 + "1.23456789",
+                                 "  r  =  1 2 3" + " " * 300 + "4", "  v  =  0.5 0.25 " + " " * 230 + "0.125",
+                                 ")Dynamics", ")Particle"]),
+    "real_system_time and roots": _j(_root(_leaf(1, "1", "0 0 0", "0 0 0"), head=["(Dynamics", "  real_system_time = 2",
+                                                                           "  system_time = 2.5", ")Dynamics"]) +
+                                     ["(Particle", "(Dynamics", "  m = 3", ")Dynamics", ")Particle", "(Particle",
+                                      ")Particle"]),
+    "unterminated last line": _j(_root(_leaf(1, "1", "1 0 0", "0 0 0")))[:-1],
 }

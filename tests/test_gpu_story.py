@@ -9,7 +9,7 @@ line number; a 262144-body snapshot.
 import numpy as np
 import pytest
 
-from story_texts import MALFORMED, flat_text, hierarchy_text
+from story_texts import MALFORMED, VARIANTS, flat_text, hierarchy_text
 
 pytestmark = pytest.mark.gpu
 
@@ -60,6 +60,13 @@ TEXTS = {
 def test_matches_oracle(name, raw, rd, so):
     text = TEXTS[name]()
     check(rd.parse(text, raw=raw), so.parse(text, raw=raw))
+
+
+@pytest.mark.parametrize("name", sorted(VARIANTS))
+def test_corner_cases_match_oracle(name, rd, so):
+    text = VARIANTS[name]
+    check(rd.parse(text), so.parse(text))
+    check(rd.parse(text, raw=True), so.parse(text, raw=True))
 
 
 def test_matches_golden(rd):

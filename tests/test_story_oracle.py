@@ -22,7 +22,7 @@ import subprocess
 import numpy as np
 import pytest
 
-from story_texts import MALFORMED, flat_text, hierarchy_text
+from story_texts import MALFORMED, VARIANTS, flat_text, hierarchy_text
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(HERE)
@@ -48,7 +48,7 @@ FIELDS = ("parent", "index", "mass", "pos", "vel", "leaves_pos", "leaves_vel", "
 
 
 def test_golden_present():
-    assert len(GOLDEN) >= 2
+    assert len(GOLDEN) >= 2 + len(VARIANTS)
 
 
 @pytest.mark.parametrize("path", GOLDEN, ids=os.path.basename)
@@ -74,6 +74,21 @@ def test_oracle_matches_reference_reader(make, so):
     named = [k for k, n in enumerate(r.names) if n is not None]
     assert [text[o.name_offset[k]:o.name_offset[k] + o.name_length[k]].decode() for k in named] == \
         [r.names[k] for k in named]
+
+
+@pytest.mark.parametrize("name", sorted(VARIANTS))
+def test_oracle_matches_reference_on_corner_cases(name, so):
+    from oracle.oracle import ref_story
+    text = VARIANTS[name]
+    r = ref_story(text)
+    if r is None:
+        pytest.skip("oracle/_ref/story_ref not built (python oracle/build_ref.py)")
+    o = so.parse(text)
+    for f in FIELDS:
+        assert same(getattr(o, f), getattr(r, f)), f
+    got = [None if o.name_offset[k] < 0 else text[o.name_offset[k]:o.name_offset[k] + o.name_length[k]].decode()
+           for k in range(o.parent.size)]
+    assert got == r.names
 
 
 def test_raw_values_are_the_written_numbers(so):
