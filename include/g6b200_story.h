@@ -24,7 +24,8 @@
  * one this reader does not convert (hexadecimal floats, NaN payloads, more
  * than 40 significant digits, section lines indented by blanks, chapters
  * inside a Dynamics/Hydro/Star section named with that section's letter),
- * parse returns -2 and g6b200_story_error names the line. */
+ * parse returns -2 and g6b200_story_error names the line.  Texts of any
+ * size below 2^31 - 2 lines (byte offsets are 64-bit). */
 #ifndef G6B200_STORY_H
 #define G6B200_STORY_H
 
@@ -45,7 +46,9 @@ typedef struct {
 
 #define G6B200_STORY_RAW 1 /* keep the values as written: no check_and_correct_node */
 
-/* A reader with its own CUDA stream and device buffers on `device`. */
+/* A reader with its own CUDA stream and device buffers on `device`, reused
+ * from one parse to the next: use a reader from one host thread at a time
+ * (one reader per thread for concurrent parses). */
 g6b200_story *g6b200_story_create(int device);
 void g6b200_story_destroy(g6b200_story *h);
 const char *g6b200_story_error(g6b200_story *h);
@@ -64,7 +67,7 @@ int g6b200_story_parse_device(g6b200_story *h, const char *d_text, long long len
  * n_roots entries. */
 int g6b200_story_nodes(g6b200_story *h, int *parent, int *index, double *mass, double (*pos)[3],
                        double (*vel)[3]);
-int g6b200_story_names(g6b200_story *h, int *name_offset, int *name_length);
+int g6b200_story_names(g6b200_story *h, long long *name_offset, int *name_length);
 int g6b200_story_leaves(g6b200_story *h, int *node, int *index, double *mass, double (*pos)[3],
                         double (*vel)[3]);
 int g6b200_story_roots(g6b200_story *h, int *root_node, double *system_time);

@@ -67,7 +67,7 @@ constexpr int kNlThreads = 256, kNlBytes = 64, kNlTile = kNlThreads * kNlBytes;
 // Line tag: code | flags | kind/key << 8 | value offset << 16.
 enum : uint32_t { C_OTHER = 0, C_OPEN = 1, C_CLOSE = 2, C_KEY = 3, C_INDENT = 4 };
 enum : uint32_t { F_EMPTY = 8, F_LONG = 16, F_STRUCT = 32 };
-enum : int { K_NONE = 0, K_M, K_R, K_V, K_TIME, K_RTIME, K_I, K_NAME, K_N, K_OTHER };
+enum : int { K_M = 1, K_R, K_V, K_TIME, K_RTIME, K_I, K_NAME, K_N, K_OTHER };  // keyword ids of key lines
 enum : int { FLD_M = 0, FLD_R, FLD_V, FLD_TIME, FLD_I, FLD_NAME, FLD_COUNT };
 
 // Error codes (low byte of the error word; the line number above it).
@@ -107,42 +107,49 @@ __device__ __forceinline__ int delta_of(uint32_t t) {
     return c == C_OPEN ? 1 : (c == C_CLOSE ? -1 : 0);
 }
 
+// Byte offsets are 64-bit (texts above 2 GB); line and node numbers 32-bit.
 struct LineRange {
-    const int *nl;
+    const long long *nl;
     int nnl;
     long long len;
-    __device__ __forceinline__ void get(int k, int &s, int &e) const {
+    __device__ __forceinline__ void get(int k, long long &s, long long &e) const {
         s = k == 0 ? 0 : nl[k - 1] + 1;
-        e = k < nnl ? nl[k] : (int)len;
+        e = k < nnl ? nl[k] : len;
+    }
+    // the line's first byte and its length after get_line's cut at 254
+    __device__ __forceinline__ int span(int k, long long &s) const {
+        long long e;
+        get(k, s, e);
+        return (int)min(e - s, (long long)kLineMax);
     }
 };
 
 // ---------------------------------------------------------------------------
 // Block scans.
 
-template <int NT>
-__device__ __forceinline__ int block_excl_sum(int v, int *total) {
-    __shared__ int ws[NT / 32];
+template <int NT, class T = int>
+__device__ __forceinline__ T block_excl_sum(T v, T *total) {
+    __shared__ T ws[NT / 32];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    int x = v;
+    T x = v;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
-        const int y = __shfl_up_sync(0xffffffffu, x, o);
+        const T y = __shfl_up_sync(0xffffffffu, x, o);
         if (lane >= o) x += y;
     }
     if (lane == 31) ws[w] = x;
     __syncthreads();
     if (w == 0) {
-        int s = lane < NT / 32 ? ws[lane] : 0;
+        T s = lane < NT / 32 ? ws[lane] : 0;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
-            const int y = __shfl_up_sync(0xffffffffu, s, o);
+            const T y = __shfl_up_sync(0xffffffffu, s, o);
             if (lane >= o) s += y;
         }
         if (lane < NT / 32) ws[lane] = s;
     }
     __syncthreads();
-    const int before = (w ? ws[w - 1] : 0) + x - v;
+    const T before = (w ? ws[w - 1] : 0) + x - v;
     if (total) *total = ws[NT / 32 - 1];
     __syncthreads();
     return before;
@@ -190,15 +197,16 @@ __global__ void __launch_bounds__(256) tile_sum_kernel(F f, long long n, int *ti
     if (threadIdx.x == 0) tile_sum[blockIdx.x] = tot;
 }
 
-__global__ void __launch_bounds__(1024) scan_tiles_kernel(int *v, int n, int *total) {
+template <class T>
+__global__ void __launch_bounds__(1024) scan_tiles_kernel(T *v, int n, T *total) {
     const int per = (n + 1023) / 1024;
     const int b = threadIdx.x * per, e = min(n, b + per);
-    int s = 0;
+    T s = 0;
     for (int k = b; k < e; ++k) s += v[k];
-    int tot;
-    int run = block_excl_sum<1024>(s, &tot);
+    T tot;
+    T run = block_excl_sum<1024, T>(s, &tot);
     for (int k = b; k < e; ++k) {
-        const int x = v[k];
+        const T x = v[k];
         v[k] = run;
         run += x;
     }
@@ -213,7 +221,7 @@ __global__ void __launch_bounds__(256) tile_apply_kernel(F f, long long n, const
         v[j] = base + j < n ? f(base + j) : 0;
         s += v[j];
     }
-    int run = block_excl_sum<256>(s, nullptr) + tile_off[blockIdx.x];
+    int run = block_excl_sum<256>(s, (int *)nullptr) + tile_off[blockIdx.x];
     for (int j = 0; j < 16; ++j)
         if (base + j < n) {
             out[base + j] = run;
@@ -252,7 +260,7 @@ __device__ __forceinline__ void load64(const char *text, long long len, long lon
     for (int i = 0; i < 4; ++i) q[i] = make_uint4(w[4 * i], w[4 * i + 1], w[4 * i + 2], w[4 * i + 3]);
 }
 
-__global__ void __launch_bounds__(kNlThreads) nl_count_kernel(const char *text, long long len, int *blk,
+__global__ void __launch_bounds__(kNlThreads) nl_count_kernel(const char *text, long long len, long long *blk,
                                                               unsigned long long *err) {
     const long long base = (long long)blockIdx.x * kNlTile + threadIdx.x * kNlBytes;
     int nl = 0;
@@ -265,11 +273,11 @@ __global__ void __launch_bounds__(kNlThreads) nl_count_kernel(const char *text, 
     if (nul) report(err, 0, E_NUL);
     int tot;
     block_excl_sum<kNlThreads>(nl, &tot);
-    if (threadIdx.x == 0) blk[blockIdx.x] = tot;
+    if (threadIdx.x == 0) blk[blockIdx.x] = (long long)tot;
 }
 
-__global__ void __launch_bounds__(kNlThreads) nl_write_kernel(const char *text, long long len, const int *blk_off,
-                                                              int *nl_pos) {
+__global__ void __launch_bounds__(kNlThreads) nl_write_kernel(const char *text, long long len,
+                                                              const long long *blk_off, long long *nl_pos) {
     const long long base = (long long)blockIdx.x * kNlTile + threadIdx.x * kNlBytes;
     int nl = 0;
     bool nul = false;
@@ -278,25 +286,29 @@ __global__ void __launch_bounds__(kNlThreads) nl_write_kernel(const char *text, 
         load64(text, len, base, q);
         for (int i = 0; i < 4; ++i) scan16(q[i], valid16(len - base - 16 * i), nl, nul);
     }
-    int o = block_excl_sum<kNlThreads>(nl, nullptr) + blk_off[blockIdx.x];
+    long long o = block_excl_sum<kNlThreads>(nl, (int *)nullptr) + blk_off[blockIdx.x];
     if (nl == 0) return;
     for (int i = 0; i < 4; ++i) {
         const uint32_t w[4] = {q[i].x, q[i].y, q[i].z, q[i].w};
         for (int j = 0; j < 16; ++j) {
             const long long pos = base + 16 * i + j;
             if (pos >= len) return;
-            if (((w[j >> 2] >> (8 * (j & 3))) & 0xffu) == '\n') nl_pos[o++] = (int)pos;
+            if (((w[j >> 2] >> (8 * (j & 3))) & 0xffu) == '\n') nl_pos[o++] = pos;
         }
     }
 }
 
 // counts: [0] newlines, [1] lines, [2] last line unterminated; the same in
-// meta[8..10], and meta[0] (end of the snapshot list) starts at the line count.
-__global__ void line_count_kernel(const char *text, long long len, const int *nnl, int *counts, int *meta) {
-    const int n = *nnl;
+// meta[8..10], and meta[0] (end of the snapshot list) starts at the line
+// count.  meta[11] = 1 when there are 2^31 - 2 lines or more (not read).
+__global__ void line_count_kernel(const char *text, long long len, const long long *nnl, int *counts, int *meta) {
+    const long long n64 = *nnl;
     const bool unterminated = len > 0 && text[len - 1] != '\n';
+    const bool too_many = n64 >= 0x7ffffffdLL;
+    const int n = too_many ? 0 : (int)n64;
+    meta[11] = too_many;
     counts[0] = meta[8] = n;
-    counts[1] = meta[9] = n + (unterminated ? 1 : 0);
+    counts[1] = meta[9] = too_many ? 0 : n + (unterminated ? 1 : 0);
     counts[2] = meta[10] = unterminated;
     meta[0] = counts[1];
 }
@@ -335,9 +347,10 @@ __global__ void classify_kernel(const char *text, LineRange lr, const int *count
     const int nlines = counts[1];
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= nlines) return;
-    int s, e;
+    long long s, e;
     lr.get(k, s, e);
-    const int full = e - s, n = min(full, kLineMax);
+    const long long full = e - s;
+    const int n = (int)min(full, (long long)kLineMax);
     const char *l = text + s;
     uint32_t t = 0;
     if (n == 0) t |= F_EMPTY;
@@ -547,7 +560,8 @@ struct NodeFlagF {
 // 6-7. Nodes, their fields, and the line checks.
 
 struct Nodes {
-    int *line, *parent, *size, *index, *name_off, *name_len, *win, *level;
+    int *line, *parent, *size, *index, *name_len, *win, *level;
+    long long *name_off;
     double *mass, *pos, *vel, *shift;
     int *shifted;
 };
@@ -610,10 +624,8 @@ __global__ void lines_kernel(const char *text, LineRange lr, const uint32_t *tag
         // Log chapters: the whole title must match (get_chapter, story.C:192-198)
         const bool log_chapter = (to & F_STRUCT) ? kind_of(to) == 'L' : (ctx[o] >= 0 && kind_of(tag[ctx[o]]) == 'L');
         if (log_chapter) {
-            int so, eo, sc, ec;
-            lr.get(o, so, eo);
-            lr.get(k, sc, ec);
-            const int no = min(eo - so, kLineMax), nc = min(ec - sc, kLineMax);
+            long long so, sc;
+            const int no = lr.span(o, so), nc = lr.span(k, sc);
             bool same = no == nc;
             for (int i = 1; same && i < no; ++i) same = text[so + i] == text[sc + i];
             if (!same) report(err, k + 1, E_TITLE);
@@ -660,29 +672,28 @@ __global__ void values_kernel(const char *text, LineRange lr, const uint32_t *ta
     if (t >= 4LL * nnodes) return;
     const int f = (int)(t / nnodes), id = (int)(t - (long long)f * nnodes);
     const int *w = N.win + FLD_COUNT * id;
-    int s, e;
+    long long s;
     if (f == 0 && w[FLD_M] >= 0) {
-        lr.get(w[FLD_M], s, e);
-        const story::Real r = story::parse_real(text + s + voff_of(tag[w[FLD_M]]), text + s + min(e - s, kLineMax));
+        const int n = lr.span(w[FLD_M], s);
+        const story::Real r = story::parse_real(text + s + voff_of(tag[w[FLD_M]]), text + s + n);
         if (r.err) report(err, w[FLD_M] + 1, E_NUMBER);
         N.mass[id] = r.v;
     }
     if (f == 1 && w[FLD_R] >= 0) {
-        lr.get(w[FLD_R], s, e);
-        if (!read_vec(text + s, min(e - s, kLineMax), N.pos + 3 * id)) report(err, w[FLD_R] + 1, E_VECTOR);
+        const int n = lr.span(w[FLD_R], s);
+        if (!read_vec(text + s, n, N.pos + 3 * id)) report(err, w[FLD_R] + 1, E_VECTOR);
     }
     if (f == 2 && w[FLD_V] >= 0) {
-        lr.get(w[FLD_V], s, e);
-        if (!read_vec(text + s, min(e - s, kLineMax), N.vel + 3 * id)) report(err, w[FLD_V] + 1, E_VECTOR);
+        const int n = lr.span(w[FLD_V], s);
+        if (!read_vec(text + s, n, N.vel + 3 * id)) report(err, w[FLD_V] + 1, E_VECTOR);
     }
     if (f == 3 && w[FLD_I] >= 0) {
-        lr.get(w[FLD_I], s, e);
-        const story::Long r = story::parse_long(text + s + voff_of(tag[w[FLD_I]]), text + s + min(e - s, kLineMax));
+        const int n = lr.span(w[FLD_I], s);
+        const story::Long r = story::parse_long(text + s + voff_of(tag[w[FLD_I]]), text + s + n);
         N.index[id] = (int)(uint32_t)(uint64_t)r.v;  // long -> int, as the reference's assignment
     }
     if (f == 3 && w[FLD_NAME] >= 0) {
-        lr.get(w[FLD_NAME], s, e);
-        const int n = min(e - s, kLineMax), a = voff_of(tag[w[FLD_NAME]]);
+        const int n = lr.span(w[FLD_NAME], s), a = voff_of(tag[w[FLD_NAME]]);
         int b = a;
         while (b < n && !c_space(text[s + b])) ++b;
         N.name_off[id] = s + a;
@@ -713,7 +724,7 @@ struct ParentF {
     __device__ int operator()(long long k) const { return size[k] > 1; }
 };
 
-__global__ void compact_kernel(long long n, const int *ex, const int *total, const int *flag_src_parent,
+__global__ void compact_kernel(long long n, const int *ex, const int *flag_src_parent,
                                const int *flag_src_size, int which, int *out) {
     const long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= n) return;
@@ -746,9 +757,9 @@ __global__ void root_time_finish_kernel(const char *text, LineRange lr, const ui
         run = max(run, root_line[roots[r]]);
         double t = 0.0;
         if (run >= 0) {
-            int s, e;
-            lr.get(run, s, e);
-            t = story::parse_real(text + s + voff_of(tag[run]), text + s + min(e - s, kLineMax)).v;
+            long long s;
+            const int n = lr.span(run, s);
+            t = story::parse_real(text + s + voff_of(tag[run]), text + s + n).v;
         }
         root_time[r] = t;
     }
@@ -935,7 +946,6 @@ class Reader {
     unsigned long long *d_err = nullptr;
     int *h_meta = nullptr;
     unsigned long long *h_err = nullptr;
-    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     template <class T>
     int ensure(int slot, T *&ptr, size_t count);
     void release();
@@ -1003,7 +1013,7 @@ int Reader::upload(const char *text, long long len, char *dst) {
 }
 
 enum Slot {
-    S_TEXT, S_BLK, S_NL, S_TAG, S_DEPTH, S_ENCL, S_CTX, S_NID, S_CHUNK, S_CHUNKBLK, S_TILES, S_TILES2, S_COUNTS,
+    S_TEXT, S_BLK, S_NLTOTAL, S_NL, S_TAG, S_DEPTH, S_ENCL, S_CTX, S_NID, S_CHUNK, S_CHUNKBLK, S_TILES, S_TILES2, S_COUNTS,
     S_NLINE, S_NPARENT, S_NSIZE, S_NINDEX, S_NNOFF, S_NNLEN, S_NWIN, S_NLEVEL, S_NMASS, S_NPOS, S_NVEL, S_NSHIFT,
     S_NSHIFTED, S_EX, S_ROOTS, S_LEAVES, S_PARENTS, S_LM, S_LX, S_LV, S_LIDX, S_RLINE, S_RTIME, S_COUNT
 };
@@ -1041,8 +1051,6 @@ void Reader::release() {
     if (d_err) cudaFree(d_err);
     if (h_meta) cudaFreeHost(h_meta);
     if (h_err) cudaFreeHost(h_err);
-    if (ev0) cudaEventDestroy(ev0);
-    if (ev1) cudaEventDestroy(ev1);
     if (stream) cudaStreamDestroy(stream);
     d_meta = nullptr;
     d_err = nullptr;
@@ -1094,8 +1102,8 @@ int Reader::sync_meta() {
 
 int Reader::parse(const char *text, long long len, bool on_device, int flags, g6b200_story_info *info) {
     if (!stream && open()) return -1;
-    if (len < 0 || len > 0x7fffff00LL) {
-        err = "story: text length outside [0, 2^31 - 256)";
+    if (len < 0) {
+        err = "story: negative text length";
         return -1;
     }
     cudaError_t e;
@@ -1121,14 +1129,20 @@ int Reader::parse(const char *text, long long len, bool on_device, int flags, g6
     cudaMemcpyAsync(d_meta, h_meta, sizeof init_meta, cudaMemcpyHostToDevice, stream);
     // 1. newline index
     const int nblk = (int)std::max<long long>(1, (len + kNlTile - 1) / kNlTile);
-    int *blk, *counts, *nl;
-    if (ensure(S_BLK, blk, (size_t)nblk) || ensure(S_COUNTS, counts, 8)) return -1;
+    long long *blk, *nl, *nl_total;
+    int *counts;
+    if (ensure(S_BLK, blk, (size_t)nblk + 1) || ensure(S_COUNTS, counts, 8) || ensure(S_NLTOTAL, nl_total, 1))
+        return -1;
     // a device text of unknown padding: read only [0, len) (the kernels stop at len; the vector loads of the
     // last 64-byte segment stay within the 16-byte-aligned allocation the caller was asked for)
     nl_count_kernel<<<nblk, kNlThreads, 0, stream>>>(d_text, len, blk, d_err);
-    scan_tiles_kernel<<<1, 1024, 0, stream>>>(blk, nblk, counts + 4);
-    line_count_kernel<<<1, 1, 0, stream>>>(d_text, len, counts + 4, counts, d_meta);
+    scan_tiles_kernel<<<1, 1024, 0, stream>>>(blk, nblk, nl_total);
+    line_count_kernel<<<1, 1, 0, stream>>>(d_text, len, nl_total, counts, d_meta);
     if (sync_meta()) return -2;
+    if (h_meta[11]) {
+        err = "story: 2^31 - 2 lines or more (not read)";
+        return -1;
+    }
     const int nnl = h_meta[8], nlines = h_meta[9];
     lines = nlines;
     if (ensure(S_NL, nl, (size_t)nnl + 1)) return -1;
@@ -1170,11 +1184,11 @@ int Reader::parse(const char *text, long long len, bool on_device, int flags, g6
     max_depth = h_meta[1];
     n_nodes = nn;
     {
-        int s_end = len > 0 ? (int)len : 0;
+        long long s_end = len > 0 ? len : 0;
         if (end_line < nlines) {
             // bytes up to the start of the line that ended the list
-            int nlpos = 0;
-            if (end_line > 0 && get_device(&nlpos, nl + end_line - 1, sizeof(int))) return -1;
+            long long nlpos = 0;
+            if (end_line > 0 && get_device(&nlpos, nl + end_line - 1, sizeof(long long))) return -1;
             s_end = end_line > 0 ? nlpos + 1 : 0;
         }
         bytes = s_end;
@@ -1212,9 +1226,9 @@ int Reader::parse(const char *text, long long len, bool on_device, int flags, g6
             return -1;
         int *d_parents;
         if (ensure(S_PARENTS, d_parents, (size_t)std::max(nparents, 1))) return -1;
-        compact_kernel<<<nbk, 256, 0, stream>>>(nn, ex, nullptr, N.parent, N.size, 0, d_roots);
-        compact_kernel<<<nbk, 256, 0, stream>>>(nn, ex + nn, nullptr, N.parent, N.size, 1, d_leaves);
-        compact_kernel<<<nbk, 256, 0, stream>>>(nn, ex + 2 * (size_t)nn, nullptr, N.parent, N.size, 2, d_parents);
+        compact_kernel<<<nbk, 256, 0, stream>>>(nn, ex, N.parent, N.size, 0, d_roots);
+        compact_kernel<<<nbk, 256, 0, stream>>>(nn, ex + nn, N.parent, N.size, 1, d_leaves);
+        compact_kernel<<<nbk, 256, 0, stream>>>(nn, ex + 2 * (size_t)nn, N.parent, N.size, 2, d_parents);
         int *rline;
         if (ensure(S_RLINE, rline, (size_t)nn) || ensure(S_RTIME, d_rtime, (size_t)std::max<long long>(n_roots, 1)))
             return -1;
@@ -1319,12 +1333,12 @@ int g6b200_story_nodes(g6b200_story *h, int *parent, int *index, double *mass, d
     return 0;
 }
 
-int g6b200_story_names(g6b200_story *h, int *name_offset, int *name_length) {
+int g6b200_story_names(g6b200_story *h, long long *name_offset, int *name_length) {
     if (!h || !h->parsed) return -1;
     storyk::Reader &r = *h->r;
     const size_t n = (size_t)r.n_nodes;
     if (n == 0) return 0;
-    if ((name_offset && r.get_device(name_offset, r.N.name_off, 4 * n)) ||
+    if ((name_offset && r.get_device(name_offset, r.N.name_off, 8 * n)) ||
         (name_length && r.get_device(name_length, r.N.name_len, 4 * n)))
         return -1;
     return 0;

@@ -134,7 +134,7 @@ class StoryReader:
         s.vel = np.empty((n, 3))
         self._check(self.lib.g6b200_story_nodes(self.h, _p(s.parent), _p(s.index), _p(s.mass), _p(s.pos), _p(s.vel)),
                     "g6b200_story_nodes")
-        s.name_offset = np.empty(n, np.int32)
+        s.name_offset = np.empty(n, np.int64)
         s.name_length = np.empty(n, np.int32)
         self._check(self.lib.g6b200_story_names(self.h, _p(s.name_offset), _p(s.name_length)), "g6b200_story_names")
         s.leaves_node = np.empty(nl, np.int32)

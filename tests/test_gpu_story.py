@@ -128,3 +128,18 @@ def test_large_snapshot(rd, so):
     assert g.info.n_leaves == 262144
     for f in ("leaves_mass", "leaves_pos", "leaves_vel", "mass", "parent"):
         assert same(getattr(g, f), getattr(o, f)), f
+
+
+def test_text_above_2gb(rd, so):
+    """Byte offsets past 2^31: 2.2 GB of Log lines ahead of the particles."""
+    head = flat_text(1000, 9)
+    k = head.index(b"(Log\n") + len(b"(Log\n")
+    filler = (b"  " + b"a" * 100 + b"\n") * 21_400_000
+    text = head[:k] + filler + head[k:]
+    del filler
+    assert len(text) > 2 ** 31 + 2 ** 25  # particle lines beyond byte 2^31
+    g = rd.parse(text)
+    o = so.parse(text)
+    assert g.info.n_leaves == 1000 and g.info.bytes == len(text)
+    for f in ("leaves_mass", "leaves_pos", "leaves_vel", "mass", "pos", "parent", "index", "system_time"):
+        assert same(getattr(g, f), getattr(o, f)), f
