@@ -284,6 +284,10 @@ def story_section(seed, n=262144, reps=10, cpu=True):
         sec = statistics.median(ts)
         out["device_raw" if raw else "device"] = {"ms": sec * 1e3, "particles_per_s": n / sec,
                                                  "text_gbs": len(text) / sec / 1e9}
+    hbm = float(measured_peaks().get("hbm_gbs", 6650.0))
+    out["roofline"] = {"bound": "per-line serial parsing (not HBM)", "achieved_text_gbs": out["device_raw"]["text_gbs"],
+                       "peak_hbm_gbs": hbm, "frac": out["device_raw"]["text_gbs"] / hbm,
+                       "peak_source": "MEASURED_PEAKS.json" if measured_peaks() else "fallback"}
     ts = []
     for _ in range(max(3, reps // 2)):
         t0 = time.perf_counter()

@@ -16,9 +16,11 @@ Errors raise ``StoryError`` with the line number.  There is no CPU path:
 without the built library or a GPU the calls fail.
 
 ``format_story`` writes a flat snapshot (a root and n leaves) laid out as
-the reference's ``put_node`` writes one (``src/node/util/tree_io.C:412+``),
-numbers with "%.18g" as ``put_real_number`` / ``put_real_vector``
-(``src/std/util_io.C:215-360``) at the default precision.
+the reference's ``put_node`` writes one (``src/node/util/tree_io.C:412+``;
+the root's Star section with the unset scale factors,
+``src/node/util/starbase_io.C:56-79``), numbers with "%.18g" as
+``put_real_number`` / ``put_real_vector`` (``src/std/util_io.C:215-360``) at
+the default precision; the root's Log holds the given lines.
 """
 import ctypes
 
@@ -172,7 +174,7 @@ def format_story(mass, pos, vel, index=None, system_time=0.0, log_lines=(), root
     out += list(log_lines)
     out += [")Log", "(Dynamics", "  system_time  =  " + _g(system_time), "  m  =  " + _g(mass.sum()),
             "  r  =  %s %s %s" % tuple(_g(c) for c in root_pos), "  v  =  0 0 0", ")Dynamics", "(Hydro", ")Hydro",
-            "(Star", ")Star"]
+            "(Star", "  mass_scale     =  -1", "  size_scale     =  -1", "  time_scale     =  -1", ")Star"]
     ms = [_g(x) for x in mass.tolist()]
     ps = [" ".join(_g(c) for c in row) for row in pos.tolist()]
     vs = [" ".join(_g(c) for c in row) for row in vel.tolist()]
