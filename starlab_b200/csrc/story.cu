@@ -774,7 +774,7 @@ __global__ void root_time_finish_kernel(const char *text, LineRange lr, const ui
 constexpr int kCorrWarps = 4;
 constexpr int kBigParent = 512;  // larger subtrees: correct_big_kernel
 constexpr int kBigTile = 1024;
-constexpr int kBigRow = kBigTile + 1;  // padded rows: the seven summing lanes read seven different banks
+constexpr int kBigRow = kBigTile + 2;  // padded rows: 16-byte aligned, the seven lanes on different banks
 constexpr size_t kBigSmem = sizeof(double) * 2 * 7 * kBigRow + sizeof(unsigned) * 2 * (kBigTile / 32);
 
 __global__ void __launch_bounds__(32 * kCorrWarps) correct_level_kernel(const int *parents, int nparents, int level,
@@ -825,7 +825,7 @@ __global__ void __launch_bounds__(32 * kCorrWarps) correct_level_kernel(const in
 // that the serial chain is one FP64 add per daughter.
 __global__ void __launch_bounds__(256) correct_big_kernel(const int *parents, int nparents, int level, int nnodes,
                                                           Nodes N) {
-    extern __shared__ double big_smem[];
+    extern __shared__ __align__(16) double big_smem[];
     double(*add)[7][kBigRow] = reinterpret_cast<double(*)[7][kBigRow]>(big_smem);
     unsigned(*mask)[kBigTile / 32] = reinterpret_cast<unsigned(*)[kBigTile / 32]>(big_smem + 2 * 7 * kBigRow);
     const int pi = blockIdx.x;
@@ -866,8 +866,17 @@ __global__ void __launch_bounds__(256) correct_big_kernel(const int *parents, in
             for (int g = 0; g < kBigTile / 32; ++g) {
                 const unsigned m = mask[b][g];
                 if (m == 0xffffffffu) {
+                    // all 32 addends into registers first, then the 32 dependent adds in order
+                    const double2 *a2 = reinterpret_cast<const double2 *>(a + 32 * g);
+                    double2 r[16];
 #pragma unroll
-                    for (int j = 0; j < 32; ++j) acc = __dadd_rn(acc, a[32 * g + j]);
+                    for (int j = 0; j < 16; ++j) r[j] = a2[j];
+                    asm volatile("" ::: "memory");  // keep the loads ahead of the dependent adds
+#pragma unroll
+                    for (int j = 0; j < 16; ++j) {
+                        acc = __dadd_rn(acc, r[j].x);
+                        acc = __dadd_rn(acc, r[j].y);
+                    }
                 } else {
                     for (unsigned bits = m; bits; bits &= bits - 1) acc = __dadd_rn(acc, a[32 * g + __ffs(bits) - 1]);
                 }

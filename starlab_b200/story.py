@@ -151,6 +151,14 @@ class StoryReader:
         self._check(self.lib.g6b200_story_roots(self.h, _p(s.root_node), _p(s.system_time)), "g6b200_story_roots")
         return s
 
+    def device_leaves(self):
+        """Device addresses of the last parse's leaf arrays (mass[n], pos[n][3],
+        vel[n][3]), valid until the next parse: for device-side consumers."""
+        m, x, v = ctypes.c_void_p(), ctypes.c_void_p(), ctypes.c_void_p()
+        self._check(self.lib.g6b200_story_device_leaves(self.h, ctypes.byref(m), ctypes.byref(x), ctypes.byref(v)),
+                    "g6b200_story_device_leaves")
+        return m.value, x.value, v.value
+
     def leaves(self, info):
         """Leaves only (mass, pos, vel), the arrays a force engine loads."""
         nl = info.n_leaves

@@ -143,3 +143,16 @@ def test_text_above_2gb(rd, so):
     assert g.info.n_leaves == 1000 and g.info.bytes == len(text)
     for f in ("leaves_mass", "leaves_pos", "leaves_vel", "mass", "pos", "parent", "index", "system_time"):
         assert same(getattr(g, f), getattr(o, f)), f
+
+
+def test_device_leaves_are_the_copied_ones(rd):
+    from cuda.bindings import runtime as rt
+    text = flat_text(3000, 12)
+    info = rd.parse_info(text)
+    m, x, v = rd.leaves(info)
+    pm, px, pv = rd.device_leaves()
+    for host, ptr in ((m, pm), (x, px), (v, pv)):
+        got = np.empty_like(host)
+        (e,) = rt.cudaMemcpy(got.ctypes.data, ptr, got.nbytes, rt.cudaMemcpyKind.cudaMemcpyDeviceToHost)
+        assert e == rt.cudaError_t.cudaSuccess
+        assert same(got, host)
