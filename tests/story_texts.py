@@ -16,7 +16,9 @@ tests and the golden-fixture script).
   blank lines, CRLF endings, tabs, chapters holding key lines inside a
   Dynamics section or a particle body, Particle-like chapters inside Log and
   Star, deep nesting, parents of zero or negative mass, every strtod /
-  strtol form, lines cut at 254 characters, an unterminated last line.
+  strtol form, lines cut at 254 characters, an unterminated last line;
+* ``random_valid_text`` -- seeded random texts the reference reads without
+  error (random trees and section orders, chapters, blank lines, CRLF).
 """
 import numpy as np
 
@@ -185,3 +187,60 @@ VARIANTS = {
                                       ")Particle"]),
     "unterminated last line": _j(_root(_leaf(1, "1", "1 0 0", "0 0 0")))[:-1],
 }
+
+
+def random_valid_text(seed):
+    """A random text the reference reads without error: random trees (the
+    Dynamics section before or after the children), chapters in Log stories,
+    Dynamics sections and particle bodies (holding key lines), repeated keys,
+    blank lines inside particles, CRLF or LF, numbers in all strtod forms."""
+    rng = np.random.default_rng(seed)
+    nl = "\r\n" if rng.random() < 0.2 else "\n"
+    out = []
+
+    def num():
+        x = float(rng.normal() * 10.0 ** rng.integers(-8, 8))
+        return _num(rng, x) if rng.random() < 0.9 else rng.choice(["0", "-0", "1.", ".5", "+2e-3", "7E+01"])
+
+    def dyn(keys=("m", "r", "v")):
+        lines = ["(Dynamics"]
+        for k in keys:
+            if rng.random() < 0.85:
+                lines.append("  %s  =  %s" % (k, num() if k == "m" else " ".join(num() for _ in range(3))))
+        if rng.random() < 0.2:
+            lines += ["(aside", "  m = %s" % num(), ")aside"]
+        if rng.random() < 0.2:
+            lines.append("  extra_key = 1 2 3")
+        lines.append(")Dynamics")
+        return lines
+
+    def node(depth):
+        lines = ["(Particle"]
+        if rng.random() < 0.8:
+            lines.append("  i = %d" % int(rng.integers(-5, 10 ** 6)))
+        if rng.random() < 0.1:
+            lines.append("  name = n%d" % int(rng.integers(0, 1000)))
+        if rng.random() < 0.1:
+            lines += ["(Note", "  i = %d" % int(rng.integers(0, 100)), ")Note"]
+        if rng.random() < 0.1:
+            lines.append("")
+        lines += ["(Log"] + (["(ch", "  text", ")ch"] if rng.random() < 0.2 else []) + [")Log"]
+        kids = int(rng.integers(2, 4)) if depth < 3 and rng.random() < 0.3 else 0
+        after = rng.random() < 0.3
+        if not after:
+            lines += dyn()
+        lines += ["(Hydro", ")Hydro", "(Star", ")Star"]
+        for _ in range(kids):
+            lines += node(depth + 1)
+        if after:
+            lines += dyn()
+        lines.append(")Particle")
+        return lines
+
+    for r in range(int(rng.integers(1, 4))):
+        root = ["(Particle", "(Log", ")Log"] + dyn(("m", "r", "v")) + (
+            ["(Dynamics", "  system_time  =  %s" % num(), ")Dynamics"] if rng.random() < 0.7 else [])
+        for _ in range(int(rng.integers(1, 12))):
+            root += node(1)
+        out += root + [")Particle"]
+    return (nl.join(out) + nl).encode()

@@ -22,7 +22,7 @@ import subprocess
 import numpy as np
 import pytest
 
-from story_texts import MALFORMED, VARIANTS, flat_text, hierarchy_text
+from story_texts import MALFORMED, VARIANTS, flat_text, hierarchy_text, random_valid_text
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(HERE)
@@ -89,6 +89,18 @@ def test_oracle_matches_reference_on_corner_cases(name, so):
     got = [None if o.name_offset[k] < 0 else text[o.name_offset[k]:o.name_offset[k] + o.name_length[k]].decode()
            for k in range(o.parent.size)]
     assert got == r.names
+
+
+def test_oracle_matches_reference_on_random_structures(so):
+    from oracle.oracle import ref_story
+    if ref_story(b"") is None:
+        pytest.skip("oracle/_ref/story_ref not built (python oracle/build_ref.py)")
+    for seed in range(60):
+        text = random_valid_text(seed)
+        r = ref_story(text)
+        o = so.parse(text)
+        for f in FIELDS:
+            assert same(getattr(o, f), getattr(r, f)), (seed, f)
 
 
 def test_raw_values_are_the_written_numbers(so):
