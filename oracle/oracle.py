@@ -306,6 +306,18 @@ def ref_story(text, path=STORY_REF, timeout=600):
     return s
 
 
+def ref_story_write(text, path=STORY_REF, timeout=600):
+    """The reference's get_dyn + put_node on text (story_ref -w): the text
+    the reference writes back, or None if the harness is not built."""
+    import subprocess
+    if not os.path.exists(path):
+        return None
+    r = subprocess.run([path, "-w"], input=text, stdout=subprocess.PIPE, stderr=subprocess.PIPE, timeout=timeout)
+    if r.returncode != 0:
+        raise RuntimeError("reference reader exited %d" % r.returncode)
+    return r.stdout
+
+
 def ref_story_seconds(path_to_text, path=STORY_REF, timeout=900):
     """Seconds the reference's get_dyn loop takes on a file (story_ref -t)."""
     import subprocess

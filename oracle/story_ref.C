@@ -12,7 +12,8 @@
 //   L x y z vx vy vz
 // and the static system time after the snapshot:  T t
 // With -t it prints nothing but the seconds spent in get_dyn and rmtree
-// (the CPU reading time of the reference).
+// (the CPU reading time of the reference); with -w it writes every snapshot
+// back with the reference's put_node (src/node/util/tree_io.C:412+).
 #include "dyn.h"
 #include <stdio.h>
 #include <string.h>
@@ -32,13 +33,16 @@ static long long dump(dyn *b, long long parent, long long &next)
 int main(int argc, char **argv)
 {
     const bool timing = argc > 1 && !strcmp(argv[1], "-t");
+    const bool write = argc > 1 && !strcmp(argv[1], "-w");
     long long next = 0, roots = 0;
     timespec t0, t1;
     clock_gettime(CLOCK_MONOTONIC, &t0);
     dyn *b;
     while ((b = get_dyn())) {
         roots++;
-        if (!timing) {
+        if (write) {
+            put_node(b);
+        } else if (!timing) {
             dump(b, -1, next);
             for_all_leaves(dyn, b, bi) {
                 if (bi == b) continue;  // for_all_leaves includes a root without daughters

@@ -103,6 +103,25 @@ def test_oracle_matches_reference_on_random_structures(so):
             assert same(getattr(o, f), getattr(r, f)), (seed, f)
 
 
+def test_format_story_writes_what_put_node_writes():
+    """starlab_b200.story.format_story against the reference's own writer: a
+    snapshot whose centre-of-mass sums are exact (equal masses, mirrored
+    dyadic positions), so get_dyn moves nothing and put_node must give the
+    same bytes back."""
+    from oracle.oracle import ref_story_write
+    from starlab_b200.story import format_story
+    n = 16
+    rng = np.random.default_rng(3)
+    half = rng.integers(-64, 65, size=(n // 2, 3)) / 32.0
+    x = np.concatenate([half, -half])
+    v = np.concatenate([half[::-1] / 4, -half[::-1] / 4])
+    text = format_story(np.full(n, 1.0 / n), x, v, log_lines=["  note = exact snapshot"])
+    back = ref_story_write(text)
+    if back is None:
+        pytest.skip("oracle/_ref/story_ref not built (python oracle/build_ref.py)")
+    assert back == text
+
+
 def test_raw_values_are_the_written_numbers(so):
     text = flat_text(50, 2)
     o = so.parse(text, raw=True)
