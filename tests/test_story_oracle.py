@@ -7,9 +7,12 @@
    check_and_correct_node, the leaves relative to their root, and the
    static system time -- and equals the committed golden vectors made by
    that reader (tests/golden/make_golden_story.py) where it is not built.
+   The same on corner-case texts and seeded random structures, and
+   format_story writes the bytes the reference's put_node writes.
 2. With raw reading the values are exactly the written numbers.
 3. Texts the reference cannot read give an error with a line number.
-4. libg6b200.so exports every entry point include/g6b200_story.h declares.
+4. libg6b200.so exports every entry point include/g6b200_story.h declares,
+   and without a GPU a reader cannot be created (no CPU path).
 """
 import ctypes
 import functools
@@ -162,3 +165,13 @@ def test_library_exports_the_story_abi():
     assert set(names) <= exported, set(names) - exported
     lib = ctypes.CDLL(LIB_PATH)
     assert all(hasattr(lib, n) for n in names)
+
+
+def test_reader_fails_loudly_without_gpu():
+    """No CPU path: without a device the reader cannot be created."""
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    from starlab_b200.story import StoryError, StoryReader
+    with pytest.raises(StoryError):
+        StoryReader()
