@@ -277,6 +277,16 @@ int g6b200_srv_wait(g6b200_server *h, long long request, double (*acc)[3], doubl
 int g6b200_srv_stats(g6b200_server *h, g6b200_srv_stats_t *out);
 void g6b200_srv_destroy(g6b200_server *h);
 
+/* Self-test of failure detection (no counterpart in the reference).  Every
+ * j-tile copy the force kernel waits for is waited on with a time bound;
+ * when a bound runs out the kernel sets a status bit and returns, and
+ * g6calc_lasthalf2_ returns 3 (kira then resets and retries).  This runs
+ * that bounded wait on a barrier nothing arrives at, through the same status
+ * word and host path: it returns 3 after about limit_ms (1 ms if <= 0), with
+ * the message in g6b200_last_error(), and the instance stays usable.  -1 on
+ * a CUDA error or while a firsthalf call is pending. */
+int g6b200_selftest_copy_timeout(int cluster_id, double limit_ms);
+
 /* Allocation-free force evaluation.  No counterpart in the reference: the
  * GRAPE-6 library owned its board memory, and this entry point exists for
  * callers of this library that cannot call cudaMalloc -- a host program

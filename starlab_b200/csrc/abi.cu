@@ -257,6 +257,14 @@ int g6b200_get_stats(int cluster_id, g6b200_stats *out) {
     return 0;
 }
 
+int g6b200_selftest_copy_timeout(int cluster_id, double limit_ms) {
+    g6::Engine *e = engine(cluster_id);
+    if (!e) return -1;
+    const int rc = e->selftest_copy_timeout(limit_ms);
+    if (rc) note(e);
+    return rc;
+}
+
 const char *g6b200_last_error(void) { return g_err.c_str(); }
 
 }  // extern "C"

@@ -854,6 +854,30 @@ int Engine::sweep(int nj, int i0, int ni, double eps2, bool copy_out, double (*a
     return 0;
 }
 
+int Engine::selftest_copy_timeout(double limit_ms) {
+    if (!open_ && open(env_int("G6B200_DEVICE", 0), 0)) return -1;
+    if (pending_) {
+        last_error = "g6b200: self-test while a firsthalf call is pending";
+        return -1;
+    }
+    G6_CHECK(cudaSetDevice(device_), "cudaSetDevice");
+    if (ensure_call_buffers(1, false, 0)) return -1;
+    G6_CHECK(cudaMemsetAsync(d_out_, 0, 16, stream_), "memset");
+    call_parity_ = 0;
+    timed_ = false;
+    launch_copy_wait_selftest(stream_, reinterpret_cast<unsigned *>(d_out_),
+                              (unsigned long long)(limit_ms > 0 ? limit_ms * 1e6 : 1e6));
+    G6_CHECK(cudaGetLastError(), "self-test launch");
+    G6_CHECK(cudaMemcpyAsync(h_out_, d_out_, 16, cudaMemcpyDeviceToHost, stream_), "status copy");
+    G6_CHECK(cudaEventRecord(ev_done_, stream_), "event");
+    const int rc = wait_call();
+    // both status words clear again for the next call, as after reset()
+    G6_CHECK(cudaMemsetAsync(d_out_, 0, 16, stream_), "memset");
+    G6_CHECK(cudaStreamSynchronize(stream_), "sync");
+    small_parity_ = 0;
+    return rc;
+}
+
 size_t Engine::footprint_bytes() const {
     return (size_t)cap_ * (sizeof(double) * JF_COUNT + sizeof(int) + kRecMax) +
            (size_t)stage_cap_ * (sizeof(double) * JF_COUNT + 2 * sizeof(int));

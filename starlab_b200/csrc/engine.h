@@ -86,6 +86,11 @@ class Engine {
     // share a launch.
     int prepare_batch_item(int nj, int ni, const double (*xi)[3], ForceParams &item, cudaEvent_t ready,
                            unsigned *status, void *dst = nullptr);
+    // Runs the force kernel's bounded copy wait against a barrier that
+    // nothing arrives at, through the same status word and wait path as a
+    // call: returns 3 (the code of a timed-out copy wait) after limit_ms,
+    // and leaves the instance ready for the next call.
+    int selftest_copy_timeout(double limit_ms);
     // After a fixed-point range report: widen the range (x4) for the next call.
     void widen_range() {
         E_ += 2;

@@ -982,4 +982,21 @@ cudaError_t launch_force(cudaStream_t s, int kmode, const ForceConfig &cfg, Forc
     return e;
 }
 
+// Self-test of the bounded wait that guards every j-tile copy: one thread
+// waits on an mbarrier that nothing arrives at and no copy completes, so
+// the wait runs out after limit_ns and the status word gets the same bit a
+// force call sets when a copy wait times out.  No copy is in flight when it
+// gives up.
+__global__ void copy_wait_selftest_kernel(unsigned *status, unsigned long long limit_ns) {
+    __shared__ __align__(8) uint64_t bar;
+    if (threadIdx.x != 0) return;
+    mbar_init(&bar, 1);
+    fence_barrier_init();
+    if (!mbar_wait_bounded(&bar, 0, limit_ns)) atomicOr(status, ST_TMA_TIMEOUT);
+}
+
+void launch_copy_wait_selftest(cudaStream_t s, unsigned *status, unsigned long long limit_ns) {
+    copy_wait_selftest_kernel<<<1, 32, 0, s>>>(status, limit_ns);
+}
+
 }  // namespace g6

@@ -206,6 +206,10 @@ cudaError_t launch_force_batch(cudaStream_t s, int kmode, const ForceConfig &cfg
                                int total_i, bool nb, bool ident);
 int batch_ctas(int kmode, const ForceConfig &cfg, int num_sms);
 
+// Self-test of the bounded copy wait: a wait on a barrier nothing arrives
+// at, which sets ST_TMA_TIMEOUT in *status after limit_ns.
+void launch_copy_wait_selftest(cudaStream_t s, unsigned *status, unsigned long long limit_ns);
+
 // Neighbour lists: per-i sort + compaction into ascending address order.
 // offsets[ni+1] (exclusive scan of min(count, cap)), out[total].
 cudaError_t launch_nb_compact(cudaStream_t s, int ni, const int *count, const int *list, int cap,
