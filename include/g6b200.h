@@ -277,6 +277,57 @@ int g6b200_srv_wait(g6b200_server *h, long long request, double (*acc)[3], doubl
 int g6b200_srv_stats(g6b200_server *h, g6b200_srv_stats_t *out);
 void g6b200_srv_destroy(g6b200_server *h);
 
+/* Potential only.  The reference computes energies through the full pair
+ * call: grape6_calculate_energies (src/node/dyn/hdyn/evolve/
+ * hdyn_grape6.C:1403-1546) drives force_by_grape(..., pot_only = true)
+ * (:474-910), which sends time 0 and unpredicted positions and reads back
+ * only pot; the ABI has no way to say so, so acc, jerk and nn are computed
+ * and discarded.  This extension runs a potential-only kernel: pot[ni] of
+ * the i-particles (index and xi as in g6calc_firsthalf_) from the j-memory
+ * predicted to the current ti.  ni <= npipes.  Blocking.  0 = OK. */
+int g6b200_calc_pot(int cluster_id, int nj, int ni, const int *index, const double (*xi)[3], double eps2,
+                    double *pot);
+/* Energies of the stored particles [0, nj) among themselves at the current
+ * ti (set ti and tj to 0 for unpredicted positions, as the reference's
+ * energy call does): epot = 1/2 sum m_i pot_i, ekin = 1/2 sum m_i |v_i|^2,
+ * both formed on the device in FP64 in a fixed order; pot [nj] is filled
+ * when not NULL.  The potential-only counterpart of the energy sums
+ * grape6_calculate_energies forms on the host (hdyn_grape6.C:1512-1527).
+ * Blocking.  0 = OK. */
+int g6b200_energies(int cluster_id, int nj, double eps2, double *epot, double *ekin, double *pot);
+
+/* One cluster's j-set split across GPUs, one process per GPU.  Counterpart
+ * of the reference's MPI force (src/node/dyn/hdyn/evolve/kira_ev.C:275-420:
+ * each rank sums over its range of j, then MPI_Allreduce SUM of acc/jerk/pot
+ * at :327-328 and MINLOC of the nearest neighbour at :409-410).  Here the
+ * global j-set is cut into blocks of block_j j (a multiple of 256); each
+ * rank holds a contiguous run of whole blocks at local addresses 0..nj-1,
+ * starting at global address j_offset.  Each block's FP64 partial sums are
+ * converted to 64-bit fixed point on a per-(i, quantity) scale all ranks
+ * agree on and summed exactly, so the results are bit-identical for any
+ * number of ranks.  The caller runs the collectives on its own stream
+ * `stream` (a cudaStream_t of this instance's device) over int64 device
+ * buffers: agree [8 ni], sums [7 ni], negj [ni].
+ *   1. g6b200_split_begin: i-block as in g6calc_firsthalf_ (index = the
+ *      i's LOCAL address, or one no local j has); returns when agree is
+ *      written.  Then all_reduce(agree, MAX).
+ *   2. g6b200_split_fix: nblocks_total = global block count.  Then
+ *      all_reduce(sums, SUM) and all_reduce(negj, MAX).
+ *   3. g6b200_split_finish: acc, jerk, pot, nn (GLOBAL address, 0 if none,
+ *      as g6calc_lasthalf2_) into host arrays; blocking.
+ * No other call on the instance between begin and finish.  In the mixed
+ * mode the ranks' fixed-point position grids must agree: every rank calls
+ * g6b200_set_position_range with the same bound on |x| first.  Returns 0 =
+ * OK. */
+int g6b200_split_begin(int cluster_id, int nj, int ni, const int *index, const double (*xi)[3],
+                       const double (*vi)[3], double eps2, int block_j, long long *agree, void *stream);
+int g6b200_split_fix(int cluster_id, long long nblocks_total, long long j_offset, const long long *agree,
+                     long long *sums, long long *negj, void *stream);
+int g6b200_split_finish(int cluster_id, long long nblocks_total, long long nj_total, const long long *agree,
+                        const long long *sums, const long long *negj, void *stream, double (*acc)[3],
+                        double (*jerk)[3], double *pot, int *nn);
+int g6b200_set_position_range(int cluster_id, double xmax);
+
 /* Self-test of failure detection (no counterpart in the reference).  Every
  * j-tile copy the force kernel waits for is waited on with a time bound;
  * when a bound runs out the kernel sets a status bit and returns, and
@@ -306,8 +357,10 @@ int g6b200_selftest_copy_timeout(int cluster_id, double limit_ms);
  * first call on a device looks up the array's device address there (with
  * that device current) and should come before any stream capture.  Calls
  * share the array: two calls whose kernels overlap on the GPU race and give
- * wrong results; order them on one stream.  Returns 0, -1 (size beyond the
- * limit), -2 (bad argument), -3 (CUDA error). */
+ * wrong results; order them on one stream.  A CUDA error already pending on
+ * the calling thread (left by earlier work) is reported as such with -3 and
+ * nothing is launched.  Returns 0, -1 (size beyond the limit), -2 (bad
+ * argument), -3 (CUDA error). */
 #define G6B200_NOALLOC_MAX_NI 32768
 int g6b200_force_noalloc(int nj, const double *xj, const double *vj,
                          const double *mj, int ni, const int *index_i,

@@ -243,6 +243,57 @@ int g6b200_sweep(int cluster_id, int nj, int i0, int ni, double eps2, double (*a
     return rc;
 }
 
+int g6b200_calc_pot(int cluster_id, int nj, int ni, const int *index, const double (*xi)[3], double eps2,
+                    double *pot) {
+    g6::Engine *e = engine(cluster_id);
+    if (!e) return -1;
+    int rc = e->potential(nj, ni, index, xi, eps2, pot);
+    if (rc) note(e);
+    return rc;
+}
+
+int g6b200_energies(int cluster_id, int nj, double eps2, double *epot, double *ekin, double *pot) {
+    g6::Engine *e = engine(cluster_id);
+    if (!e) return -1;
+    int rc = e->energies(nj, eps2, epot, ekin, pot);
+    if (rc) note(e);
+    return rc;
+}
+
+int g6b200_split_begin(int cluster_id, int nj, int ni, const int *index, const double (*xi)[3],
+                       const double (*vi)[3], double eps2, int block_j, long long *agree, void *stream) {
+    g6::Engine *e = engine(cluster_id);
+    if (!e) return -1;
+    int rc = e->split_begin(nj, ni, index, xi, vi, eps2, block_j, agree, stream);
+    if (rc) note(e);
+    return rc;
+}
+
+int g6b200_split_fix(int cluster_id, long long nblocks_total, long long j_offset, const long long *agree,
+                     long long *sums, long long *negj, void *stream) {
+    g6::Engine *e = engine(cluster_id);
+    if (!e) return -1;
+    int rc = e->split_fix(nblocks_total, j_offset, agree, sums, negj, stream);
+    if (rc) note(e);
+    return rc;
+}
+
+int g6b200_split_finish(int cluster_id, long long nblocks_total, long long nj_total, const long long *agree,
+                        const long long *sums, const long long *negj, void *stream, double (*acc)[3],
+                        double (*jerk)[3], double *pot, int *nn) {
+    g6::Engine *e = engine(cluster_id);
+    if (!e) return -1;
+    int rc = e->split_finish(nblocks_total, nj_total, agree, sums, negj, stream, acc, jerk, pot, nn);
+    if (rc) note(e);
+    return rc;
+}
+
+int g6b200_set_position_range(int cluster_id, double xmax) {
+    g6::Engine *e = engine(cluster_id, false);
+    e->set_position_range(xmax);
+    return 0;
+}
+
 int g6b200_get_stats(int cluster_id, g6b200_stats *out) {
     const g6::EngineStats &s = engine(cluster_id, false)->stats();
     out->calls = s.calls;

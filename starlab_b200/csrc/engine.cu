@@ -117,6 +117,7 @@ int Engine::open(int device, int nmax_hint) {
     G6_CHECK(cudaDeviceGetAttribute(&num_sms_, cudaDevAttrMultiProcessorCount, device_), "attr");
     cudaEvent_t *evs[] = {&ev_stage_, &ev_begin_, &ev_pred0_, &ev_pred1_, &ev_force0_, &ev_force1_, &ev_done_};
     for (cudaEvent_t *e : evs) G6_CHECK(cudaEventCreate(e), "event");
+    G6_CHECK(cudaEventCreateWithFlags(&ev_ext_, cudaEventDisableTiming), "event");
     stage_cap_ = 16384;
     G6_CHECK(cudaMallocHost(&h_stage_vals_, sizeof(double) * JF_COUNT * stage_cap_), "pinned stage");
     G6_CHECK(cudaMallocHost(&h_stage_addr_, sizeof(int) * stage_cap_), "pinned stage");
@@ -124,6 +125,8 @@ int Engine::open(int device, int nmax_hint) {
     G6_CHECK(cudaMalloc(&d_stage_vals_, sizeof(double) * JF_COUNT * stage_cap_), "stage");
     G6_CHECK(cudaMalloc(&d_stage_addr_, sizeof(int) * stage_cap_), "stage");
     G6_CHECK(cudaMalloc(&d_stage_index_, sizeof(int) * stage_cap_), "stage");
+    G6_CHECK(cudaMalloc(&d_energy_, sizeof(double) * (2 * kEnergyBlocks + 2)), "energy");
+    G6_CHECK(cudaMallocHost(&h_energy_, sizeof(double) * 2), "energy");
     open_ = true;
     if (ensure_capacity(std::max(nmax_hint, 1024) - 1)) return -1;
     return 0;
@@ -134,9 +137,9 @@ void Engine::close() {
     if (getenv("G6B200_TRACE")) {
         fprintf(stderr,
                 "g6b200[%d] trace: calls %lld interactions %lld launches %lld predictions %lld nb_calls %lld "
-                "range_retries %lld grows %lld wait_ms %.1f host_ms %.1f mode %d\n",
+                "pair_calls %lld range_retries %lld grows %lld wait_ms %.1f host_ms %.1f mode %d\n",
                 cluster_id_, stats_.calls, stats_.interactions, stats_.launches, stats_.predictions, stats_.nb_calls,
-                stats_.range_retries, stats_.grows, stats_.wait_ms, stats_.host_ms, mode_);
+                stats_.pair_calls, stats_.range_retries, stats_.grows, stats_.wait_ms, stats_.host_ms, mode_);
     }
     cudaSetDevice(device_);
     cudaStreamSynchronize(stream_);
@@ -148,9 +151,11 @@ void Engine::close() {
     dfree(d_nb_count_); dfree(d_nb_list_); dfree(d_nb_sorted_); dfree(d_nb_off_); dfree(d_bulk_);
     hfree(h_stage_vals_); hfree(h_stage_addr_); hfree(h_stage_index_);
     hfree(h_irec_); hfree(h_out_); hfree(h_nb_off_); hfree(h_nb_count_); hfree(h_bulk_);
-    hfree(h_ieps2_); dfree(d_ieps2_);
+    hfree(h_ieps2_); dfree(d_ieps2_); hfree(h_energy_); dfree(d_energy_);
     cudaEvent_t evs[] = {ev_stage_, ev_begin_, ev_pred0_, ev_pred1_, ev_force0_, ev_force1_, ev_done_};
     for (cudaEvent_t e : evs) if (e) cudaEventDestroy(e);
+    if (ev_ext_) cudaEventDestroy(ev_ext_);
+    ev_ext_ = nullptr;
     cudaStreamDestroy(stream_);
     d_jraw_ = nullptr; d_jindex_ = nullptr; d_jrec_ = nullptr;
     d_stage_vals_ = nullptr; d_stage_addr_ = nullptr; d_stage_index_ = nullptr;
@@ -160,7 +165,7 @@ void Engine::close() {
     h_bulk_ = nullptr; h_bulk_cap_ = 0; bulk_busy_ = false;
     h_stage_vals_ = nullptr; h_stage_addr_ = nullptr; h_stage_index_ = nullptr;
     h_irec_ = nullptr; h_out_ = nullptr; h_nb_off_ = nullptr; h_nb_count_ = nullptr;
-    h_ieps2_ = nullptr; d_ieps2_ = nullptr;
+    h_ieps2_ = nullptr; d_ieps2_ = nullptr; h_energy_ = nullptr; d_energy_ = nullptr;
     ev_stage_ = ev_begin_ = ev_pred0_ = ev_pred1_ = ev_force0_ = ev_force1_ = ev_done_ = nullptr;
     stream_ = nullptr;
     cap_ = 0; call_cap_ = 0; part_cap_ = 0; nb_alloc_ = 0;
@@ -567,13 +572,17 @@ int Engine::firsthalf_impl(int nj, int ni, const int *index, const double (*xi)[
     double xm = xmax_;
     for (double m : tmax) xm = std::max(xm, m);
     xmax_ = xm;
+    if (ni == 2 && index && index[0] == index[1]) stats_.pair_calls++;
     call_ni_ = ni;
     call_nj_ = nj;
     call_eps2_ = eps2;
     call_nb_ = nb;
     call_g4_ = ieps2 != nullptr;
     call_sweep_ = false;
-    call_copy_ = true;
+    call_pot_ = pot_request_;
+    call_energy_ = false;
+    call_split_ = split_request_;
+    call_copy_ = call_split_ == 0;  // a split call's results stay on the device
     call_i0_ = 0;
     nb_read_ = false;
     // The one-launch form pays for its 14 KB parameter block by replacing the
@@ -696,7 +705,14 @@ int Engine::launch_call() {
             }
         }
         ForceConfig cfg = override_.il > 0 ? override_ : choose_config(km, ni, nj_pad, num_sms_, call_nb_);
-        if (ensure_call_buffers(ni, call_nb_, partial_bytes(cfg, ni))) return -1;
+        // Potential-only kernel (one i per thread) for the paired mixed and
+        // FP64 layouts; the scalar mixed layout runs its full kernel.
+        const bool pot_k = call_pot_ && km != kKernMixedDS;
+        if (pot_k) cfg.r = 1;
+        if (call_split_) cfg.jper = call_split_;
+        if (ensure_call_buffers(ni, call_nb_, call_split_ ? partial_bytes_fixed(call_split_, nj_pad, ni)
+                                                          : partial_bytes(cfg, ni)))
+            return -1;
         last_cfg_ = cfg;
         ForceParams p{};
         p.jrec = d_jrec_;
@@ -716,14 +732,29 @@ int Engine::launch_call() {
         p.nb_cap = nb_cap_;
         p.include_self = npipes_ > 48;
         p.status = status;
-        p.tile_counter = d_tile_cnt_;
+        p.tile_counter = call_split_ ? nullptr : d_tile_cnt_;
         p.ieps2 = call_g4_ ? d_ieps2_ : nullptr;
+        p.keep_partials = call_split_ ? 1 : 0;
         if (call_nb_) G6_CHECK(cudaMemsetAsync(d_nb_count_, 0, sizeof(int) * ni, stream_), "memset");
         if (timed_) G6_CHECK(cudaEventRecord(ev_force0_, stream_), "event");
-        G6_CHECK(launch_force(stream_, km, cfg, p, n_nonident_ == 0 && !call_g4_, call_nb_, call_g4_),
+        G6_CHECK(launch_force(stream_, km, cfg, p, n_nonident_ == 0 && !call_g4_, call_nb_, call_g4_, pot_k),
                  "force launch");
         if (timed_) G6_CHECK(cudaEventRecord(ev_force1_, stream_), "event");
         stats_.launches += 1;
+        if (call_split_) {
+            split_nsplit_ = std::max(1, (nj_pad + call_split_ - 1) / call_split_);
+            launch_split_agree(stream_, ni, split_nsplit_, d_part_, split_agree_);
+            G6_CHECK(cudaGetLastError(), "split launch");
+            stats_.launches++;
+        }
+        if (call_energy_) {
+            launch_energy(stream_, ni, call_i0_, d_irec_, d_jraw_, cap_, p.out_pot, d_energy_);
+            G6_CHECK(cudaGetLastError(), "energy launch");
+            stats_.launches += 2;
+            G6_CHECK(cudaMemcpyAsync(h_energy_, d_energy_ + 2 * kEnergyBlocks, 2 * sizeof(double),
+                                     cudaMemcpyDeviceToHost, stream_), "energy copy");
+            stats_.d2h_bytes += 2 * (long long)sizeof(double);
+        }
         if (call_nb_) {
             stats_.nb_calls++;
             G6_CHECK(launch_nb_compact(stream_, ni, d_nb_count_, d_nb_list_, nb_cap_, d_nb_off_, d_nb_sorted_),
@@ -837,6 +868,9 @@ int Engine::sweep(int nj, int i0, int ni, double eps2, bool copy_out, double (*a
     call_g4_ = false;
     call_small_ = false;
     call_sweep_ = true;
+    call_pot_ = false;
+    call_energy_ = false;
+    call_split_ = 0;
     call_copy_ = copy_out;
     call_i0_ = i0;
     nb_read_ = false;
@@ -851,6 +885,139 @@ int Engine::sweep(int nj, int i0, int ni, double eps2, bool copy_out, double (*a
         if (pot) memcpy(pot, h_out_ + L.pot, 8 * (size_t)ni);
         if (nn) memcpy(nn, h_out_ + L.nn, 4 * (size_t)ni);
     }
+    return 0;
+}
+
+int Engine::potential(int nj, int ni, const int *index, const double (*xi)[3], double eps2, double *pot) {
+    if (pending_) {
+        last_error = "g6b200: potential call while a firsthalf call is pending";
+        return -1;
+    }
+    std::vector<double> zv(3 * (size_t)std::max(ni, 1), 0.0);  // the potential needs no velocities
+    pot_request_ = true;
+    int rc = firsthalf_impl(nj, ni, index, xi, reinterpret_cast<const double (*)[3]>(zv.data()), eps2, nullptr,
+                            nullptr);
+    pot_request_ = false;
+    if (rc) return rc;
+    return lasthalf(ni, nullptr, nullptr, pot, nullptr);
+}
+
+int Engine::energies(int nj, double eps2, double *epot, double *ekin, double *pot) {
+    if (pending_) {
+        last_error = "g6b200: energy call while a firsthalf call is pending";
+        return -1;
+    }
+    if (!open_ && open(env_int("G6B200_DEVICE", 0), 0)) return -1;
+    if (nj < 0) {
+        last_error = "g6b200: bad energy call size";
+        return -1;
+    }
+    G6_CHECK(cudaSetDevice(device_), "cudaSetDevice");
+    if (nj > 0 && ensure_capacity(nj - 1)) return -1;
+    if (ensure_call_buffers(nj, false, 0)) return -1;
+    call_ni_ = nj;
+    call_nj_ = nj;
+    call_eps2_ = eps2;
+    call_nb_ = false;
+    call_g4_ = false;
+    call_small_ = false;
+    call_sweep_ = true;
+    call_pot_ = true;
+    call_energy_ = nj > 0;
+    call_split_ = 0;
+    call_copy_ = pot != nullptr;
+    call_i0_ = 0;
+    nb_read_ = false;
+    int rc = flush_j() || launch_call() ? -1 : wait_call();
+    call_energy_ = false;
+    call_pot_ = false;
+    if (rc) return rc;
+    if (epot) *epot = nj > 0 ? h_energy_[0] : 0.0;
+    if (ekin) *ekin = nj > 0 ? h_energy_[1] : 0.0;
+    if (pot) memcpy(pot, h_out_ + OutLayout(nj).pot, 8 * (size_t)nj);
+    return 0;
+}
+
+void Engine::set_position_range(double xmax) {
+    if (xmax > xmax_) xmax_ = xmax;
+    const int E = std::max(E_, choose_E(xmax_));
+    if (E != E_) {
+        E_ = E;
+        pred_valid_ = false;
+    }
+}
+
+int Engine::split_begin(int nj, int ni, const int *index, const double (*xi)[3], const double (*vi)[3],
+                        double eps2, int block_j, long long *agree, void *stream) {
+    if (pending_) {
+        last_error = "g6b200: split call while a firsthalf call is pending";
+        return -1;
+    }
+    if (block_j <= 0 || block_j % 256 || !agree) {
+        last_error = "g6b200: split call needs block_j a positive multiple of 256 and an agree buffer";
+        return -1;
+    }
+    if (!open_ && open(env_int("G6B200_DEVICE", 0), 0)) return -1;
+    G6_CHECK(cudaSetDevice(device_), "cudaSetDevice");
+    // the caller's earlier work on `agree` comes first
+    G6_CHECK(cudaEventRecord(ev_ext_, static_cast<cudaStream_t>(stream)), "event");
+    G6_CHECK(cudaStreamWaitEvent(stream_, ev_ext_, 0), "stream wait");
+    split_request_ = block_j;
+    split_agree_ = agree;
+    int rc = firsthalf_impl(nj, ni, index, xi, vi, eps2, nullptr, nullptr);
+    split_request_ = 0;
+    if (rc) return rc;
+    pending_ = false;
+    rc = wait_call();  // also retries a fixed-point range report (agree is rewritten)
+    call_split_ = 0;
+    return rc;
+}
+
+int Engine::split_fix(long long nblocks_total, long long j_offset, const long long *agree, long long *sums,
+                      long long *negj, void *stream) {
+    if (split_nsplit_ <= 0) {
+        last_error = "g6b200: split_fix without a split_begin";
+        return -1;
+    }
+    G6_CHECK(cudaSetDevice(device_), "cudaSetDevice");
+    cudaStream_t cs = static_cast<cudaStream_t>(stream);
+    G6_CHECK(cudaEventRecord(ev_ext_, cs), "event");
+    G6_CHECK(cudaStreamWaitEvent(stream_, ev_ext_, 0), "stream wait");
+    launch_split_fix(stream_, call_ni_, split_nsplit_, split_log2_blocks(nblocks_total), j_offset, d_part_, agree,
+                     sums, negj);
+    G6_CHECK(cudaGetLastError(), "split fix launch");
+    stats_.launches++;
+    G6_CHECK(cudaEventRecord(ev_ext_, stream_), "event");
+    G6_CHECK(cudaStreamWaitEvent(cs, ev_ext_, 0), "stream wait");
+    return 0;
+}
+
+int Engine::split_finish(long long nblocks_total, long long nj_total, const long long *agree, const long long *sums,
+                         const long long *negj, void *stream, double (*acc)[3], double (*jerk)[3], double *pot,
+                         int *nn) {
+    if (split_nsplit_ <= 0) {
+        last_error = "g6b200: split_finish without a split_begin";
+        return -1;
+    }
+    G6_CHECK(cudaSetDevice(device_), "cudaSetDevice");
+    G6_CHECK(cudaEventRecord(ev_ext_, static_cast<cudaStream_t>(stream)), "event");
+    G6_CHECK(cudaStreamWaitEvent(stream_, ev_ext_, 0), "stream wait");
+    const int ni = call_ni_;
+    OutLayout L(ni);
+    launch_split_finish(stream_, ni, split_log2_blocks(nblocks_total), nj_total, agree, sums, negj,
+                        reinterpret_cast<double *>(d_out_ + L.acc), reinterpret_cast<double *>(d_out_ + L.jerk),
+                        reinterpret_cast<double *>(d_out_ + L.pot), reinterpret_cast<int *>(d_out_ + L.nn));
+    G6_CHECK(cudaGetLastError(), "split finish launch");
+    stats_.launches++;
+    G6_CHECK(cudaMemcpyAsync(h_out_ + L.acc, d_out_ + L.acc, L.total - L.acc, cudaMemcpyDeviceToHost, stream_),
+             "out copy");
+    stats_.d2h_bytes += (long long)(L.total - L.acc);
+    G6_CHECK(cudaStreamSynchronize(stream_), "sync");
+    split_nsplit_ = 0;
+    if (acc) memcpy(acc, h_out_ + L.acc, 24 * (size_t)ni);
+    if (jerk) memcpy(jerk, h_out_ + L.jerk, 24 * (size_t)ni);
+    if (pot) memcpy(pot, h_out_ + L.pot, 8 * (size_t)ni);
+    if (nn) memcpy(nn, h_out_ + L.nn, 4 * (size_t)ni);
     return 0;
 }
 

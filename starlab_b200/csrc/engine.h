@@ -19,6 +19,10 @@ struct EngineStats {
     long long launches = 0;  // kernels launched by this instance
     // diagnostics (G6B200_TRACE=1 prints them when the instance closes)
     long long range_retries = 0, nb_calls = 0, predictions = 0, grows = 0;
+    // calls of two i sharing one index: kira's binary perturbation call
+    // (hdyn_grape6.C:3415-3587 sends both components with their top-level
+    // node's index)
+    long long pair_calls = 0;
     double wait_ms = 0, host_ms = 0;
 };
 
@@ -66,6 +70,31 @@ class Engine {
     // copy_out false the results stay in device memory.
     int sweep(int nj, int i0, int ni, double eps2, bool copy_out, double (*acc)[3], double (*jerk)[3],
               double *pot, int *nn);
+    // Potential only (no acc, jerk, nn): pot[ni] of the i-particles at the
+    // j-memory predicted to the current ti.  Blocking.  ni <= npipes.
+    int potential(int nj, int ni, const int *index, const double (*xi)[3], double eps2, double *pot);
+    // Energies of the stored particles [0, nj) among themselves at the
+    // current ti: epot = 1/2 sum m_i pot_i, ekin = 1/2 sum m_i |v_i|^2 (FP64,
+    // fixed summation order), pot[nj] optionally copied out.  Blocking.
+    int energies(int nj, double eps2, double *epot, double *ekin, double *pot);
+    // Multi-GPU j-split of one cluster (split.cu; the caller runs the
+    // collectives between the steps on `stream`, a cudaStream_t of this
+    // device).  begin: force on the i-block from this instance's j-slice with
+    // the slice cut into splits of block_j j (a multiple of 256), every
+    // split's partial sums kept; writes agree[8 ni] (int64, device) and
+    // returns when it is written.  fix: after the MAX all-reduce of agree,
+    // sums[7 ni] and negj[ni] (int64, device) for the SUM / MAX all-reduces;
+    // j_offset is the slice's first global address.  finish: the FP64
+    // results from the reduced buffers, copied to host arrays (blocking).
+    int split_begin(int nj, int ni, const int *index, const double (*xi)[3], const double (*vi)[3], double eps2,
+                    int block_j, long long *agree, void *stream);
+    int split_fix(long long nblocks_total, long long j_offset, const long long *agree, long long *sums,
+                  long long *negj, void *stream);
+    int split_finish(long long nblocks_total, long long nj_total, const long long *agree, const long long *sums,
+                     const long long *negj, void *stream, double (*acc)[3], double (*jerk)[3], double *pot, int *nn);
+    // Widen the mixed mode's fixed-point range to hold |x| <= xmax (ranks
+    // of a split cluster pass the same value, so their grids agree).
+    void set_position_range(double xmax);
     int read_neighbours();
     int get_neighbours(int pipe, int max_length, int *nblen, int *nbl);
     // Neighbour count of a pipe of the last call (after read_neighbours).
@@ -199,7 +228,17 @@ class Engine {
     int call_parity_ = 0;   // status word of the call in flight
     bool call_error_ = false;
     bool call_sweep_ = false;
+    bool pot_request_ = false;  // the next firsthalf_impl call is a potential() call
+    int split_request_ = 0;     // > 0: the next firsthalf_impl call is a split_begin() (block_j)
+    int call_split_ = 0;        // block_j of the split call in flight (0: none)
+    int split_nsplit_ = 0;      // splits of the last split call
+    long long *split_agree_ = nullptr;  // caller's agree buffer of the split call
+    cudaEvent_t ev_ext_ = nullptr;      // ordering against the caller's stream
+    bool call_pot_ = false;     // potential-only kernel
+    bool call_energy_ = false;  // + the energy reduction (sweeps)
     bool call_copy_ = true;
+    double *d_energy_ = nullptr;  // [2 * kEnergyBlocks + 2] block partials, then epot, ekin
+    double *h_energy_ = nullptr;  // pinned: epot, ekin
     int call_i0_ = 0;
     ForceConfig last_cfg_{};
     cudaEvent_t ev_begin_ = nullptr, ev_pred0_ = nullptr, ev_pred1_ = nullptr;

@@ -41,7 +41,10 @@
 namespace g6 {
 
 constexpr uint64_t kWaitLimitNs = 1000000000ull;  // 1 s per tile wait
-constexpr int kFlush = 64;                        // FP32 terms per FP64 fold
+#ifndef G6B200_FOLD_TERMS
+#define G6B200_FOLD_TERMS 64
+#endif
+constexpr int kFlush = G6B200_FOLD_TERMS;         // FP32 terms per FP64 fold
 constexpr int kMaxWarps = 8;
 
 // T j per shared-memory tile, held as U records of JPU j each.
@@ -197,9 +200,24 @@ __device__ __forceinline__ void interact_mixed(S &s, const JMixed &J, int jg, fl
     }
 }
 
-template <bool CHK, bool NB, bool IDENT, bool G4 = false>
+template <bool CHK, bool NB, bool IDENT, bool G4 = false, bool PO = false>
 __device__ __forceinline__ void interact(StateF64 &s, const double4 &pos, const double4 &vel,
                                          int jg, double eps2, const ForceParams &p) {
+    if constexpr (PO) {
+        // Potential only: the pot term of the full form below.
+        const double dx = pos.x - s.x;
+        const double dy = pos.y - s.y;
+        const double dz = pos.z - s.z;
+        double r2 = dx * dx + dy * dy + dz * dz + eps2;
+        double mj = pos.w;
+        if (CHK) {
+            const bool self = IDENT ? (jg == s.idx) : ((int)vel.w == s.idx);
+            r2 = self ? 1.0 : r2;
+            mj = self ? 0.0 : mj;
+        }
+        s.Pt -= mj * rsqrt(r2);
+        return;
+    }
     const double dx = pos.x - s.x;
     const double dy = pos.y - s.y;
     const double dz = pos.z - s.z;
@@ -303,9 +321,35 @@ __device__ __forceinline__ void load_i(StateMixedP &s, const IRec &q, const Forc
     s.nj = -1;
 }
 
-template <bool CHK, bool NB, bool IDENT>
+template <bool CHK, bool NB, bool IDENT, bool PO = false>
 __device__ __forceinline__ void interact_pair(StateMixedP &s, const JPairMixed &J, int jg0, float2 eps2,
                                               const ForceParams &p) {
+    if constexpr (PO) {
+        // Potential only: the exact position difference, r^2, the refined
+        // inverse distance and m/r -- the pot terms of the full form below,
+        // rounded identically.
+        const float2 dx = __fadd2_rn(__fadd2_rn(make_float2(J.hxy.x, J.hxy.y), s.nxh),
+                                     __fadd2_rn(make_float2(J.lxy.x, J.lxy.y), s.nxl));
+        const float2 dy = __fadd2_rn(__fadd2_rn(make_float2(J.hxy.z, J.hxy.w), s.nyh),
+                                     __fadd2_rn(make_float2(J.lxy.z, J.lxy.w), s.nyl));
+        const float2 dz = __fadd2_rn(__fadd2_rn(make_float2(J.hzm.x, J.hzm.y), s.nzh),
+                                     __fadd2_rn(make_float2(J.lzi.x, J.lzi.y), s.nzl));
+        float2 r2 = __fadd2_rn(__ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __fmul2_rn(dx, dx))), eps2);
+        float2 m = make_float2(J.hzm.z, J.hzm.w);
+        if (CHK) {
+            const bool self0 = IDENT ? (jg0 == s.idx) : (__float_as_int(J.lzi.z) == s.idx);
+            const bool self1 = IDENT ? (jg0 + 1 == s.idx) : (__float_as_int(J.lzi.w) == s.idx);
+            r2.x = self0 ? 1.f : r2.x;
+            r2.y = self1 ? 1.f : r2.y;
+            m.x = self0 ? 0.f : m.x;
+            m.y = self1 ? 0.f : m.y;
+        }
+        float2 y = make_float2(rsqrt_approx(r2.x), rsqrt_approx(r2.y));
+        const float2 ry = __fmul2_rn(r2, y);
+        y = __fmul2_rn(y, __ffma2_rn(ry, y, dup(-3.f)));
+        s.pm = __fadd2_rn(s.pm, __fmul2_rn(m, y));
+        return;
+    }
     const float2 dx = __fadd2_rn(__fadd2_rn(make_float2(J.hxy.x, J.hxy.y), s.nxh),
                                  __fadd2_rn(make_float2(J.lxy.x, J.lxy.y), s.nxl));
     const float2 dy = __fadd2_rn(__fadd2_rn(make_float2(J.hxy.z, J.hxy.w), s.nyh),
@@ -378,6 +422,19 @@ __device__ __forceinline__ void fold(StateMixedP &s) {
     s.ax = s.ay = s.az = s.jx = s.jy = s.jz = s.pm = make_float2(0.f, 0.f);
 }
 
+__device__ __forceinline__ void fold_pot(StateMixedP &s) {
+    s.Pt -= 4.0 * (double)s.pm.x; s.Pt -= 4.0 * (double)s.pm.y;  // pm sums m/(4r)
+    s.pm = make_float2(0.f, 0.f);
+}
+
+template <bool PO>
+__device__ __forceinline__ void fold_any(StateMixedP &s) {
+    if constexpr (PO)
+        fold_pot(s);
+    else
+        fold(s);
+}
+
 __device__ __forceinline__ void fold(StateMixedBase &s) {
     s.Ax += (double)s.ax;
     s.Ay += (double)s.ay;
@@ -395,6 +452,8 @@ __device__ __forceinline__ void fold(StateMixedBase &s) {
 constexpr int kVarUnroll4 = 2;
 // 4 = GRAPE-4 pipeline (FP64 kernel only; see the file header).
 constexpr int kVarG4 = 4;
+// 8 = potential only (paired mixed and FP64 layouts): the energy sweeps.
+constexpr int kVarPot = 8;
 
 // Consume one shared-memory tile: this thread's j are kbase + m*JL.
 template <int K, int R, int JL, bool CHK, bool NB, bool IDENT, int V>
@@ -402,29 +461,39 @@ __device__ __forceinline__ void consume_tile(typename StateOf<K>::type (&st)[R],
                                              const typename Traits<K>::JRec *S, int kbase,
                                              int per, int tb, const ForceParams &p) {
     if constexpr (K == kKernMixedP) {
+        constexpr bool PO = (V & kVarPot) != 0;
         const float2 eps2 = dup((float)p.eps2);
         constexpr int kFlushPairs = kFlush / 2;
+        if constexpr (kFlushPairs <= 2) {
+            // Short folds: every one or two pair records go into FP64.
+#pragma unroll 4
+            for (int m = 0; m < per; m += kFlushPairs) {
+#pragma unroll
+                for (int u = 0; u < kFlushPairs; ++u) {
+                    if (u == 0 || m + u < per) {
+                        const int k = kbase + (m + u) * JL;
+                        const JPairMixed J = S[k];
+#pragma unroll
+                        for (int r = 0; r < R; ++r)
+                            interact_pair<CHK, NB, IDENT, PO>(st[r], J, tb + 2 * k, eps2, p);
+                    }
+                }
+#pragma unroll
+                for (int r = 0; r < R; ++r) fold_any<PO>(st[r]);
+            }
+            return;
+        }
         for (int m0 = 0; m0 < per; m0 += kFlushPairs) {
             const int m1 = min(m0 + kFlushPairs, per);
-            if (V & kVarUnroll4) {
 #pragma unroll 4
-                for (int m = m0; m < m1; ++m) {
-                    const int k = kbase + m * JL;
-                    const JPairMixed J = S[k];
+            for (int m = m0; m < m1; ++m) {
+                const int k = kbase + m * JL;
+                const JPairMixed J = S[k];
 #pragma unroll
-                    for (int r = 0; r < R; ++r) interact_pair<CHK, NB, IDENT>(st[r], J, tb + 2 * k, eps2, p);
-                }
-            } else {
-#pragma unroll 2
-                for (int m = m0; m < m1; ++m) {
-                    const int k = kbase + m * JL;
-                    const JPairMixed J = S[k];
-#pragma unroll
-                    for (int r = 0; r < R; ++r) interact_pair<CHK, NB, IDENT>(st[r], J, tb + 2 * k, eps2, p);
-                }
+                for (int r = 0; r < R; ++r) interact_pair<CHK, NB, IDENT, PO>(st[r], J, tb + 2 * k, eps2, p);
             }
 #pragma unroll
-            for (int r = 0; r < R; ++r) fold(st[r]);
+            for (int r = 0; r < R; ++r) fold_any<PO>(st[r]);
         }
     } else if constexpr (K == kKernF64) {
         const double eps2 = p.eps2;
@@ -435,7 +504,7 @@ __device__ __forceinline__ void consume_tile(typename StateOf<K>::type (&st)[R],
             const double4 vel = S[k].vel;
 #pragma unroll
             for (int r = 0; r < R; ++r)
-                interact<CHK, NB, IDENT, (V & kVarG4) != 0>(st[r], pos, vel, tb + k, eps2, p);
+                interact<CHK, NB, IDENT, (V & kVarG4) != 0, (V & kVarPot) != 0>(st[r], pos, vel, tb + k, eps2, p);
         }
     } else {
         const float eps2 = (float)p.eps2;
@@ -565,7 +634,7 @@ template <int K, int R> struct MinBlocks {
 // ring stage and the mbarrier phase, so a persistent CTA can run many
 // tasks back to back).
 template <int K, int IL, int R, bool NB, bool IDENT, int V>
-__device__ __forceinline__ void process_task(const ForceParams &p, int itile_idx, int split, unsigned char *smem,
+__device__ __forceinline__ bool process_task(const ForceParams &p, int itile_idx, int split, unsigned char *smem,
                                              int &gt) {
     using Tr = Traits<K>;
     using JRec = typename Tr::JRec;
@@ -620,14 +689,15 @@ __device__ __forceinline__ void process_task(const ForceParams &p, int itile_idx
     const int per = U / (H * JL);
     const int kbase = h * (U / H) + jl;
     bool ok = true;
-    for (int t = 0; t < ntiles; ++t) {
+    int t = 0;
+    for (; t < ntiles; ++t) {
         const int gg = g0 + t;
         const int b = gg & 1;
         if (threadIdx.x == 0 && t + 1 < ntiles) {
             mbar_arrive_expect_tx(&bars[b ^ 1], kTileBytes);
             bulk_g2s(tiles + (b ^ 1) * U, jrec + (jb + (t + 1) * T) / JPU, kTileBytes, &bars[b ^ 1]);
         }
-        if (ok) ok = mbar_wait_bounded(&bars[b], (gg >> 1) & 1, kWaitLimitNs);
+        const bool arrived = mbar_wait_bounded(&bars[b], (gg >> 1) & 1, kWaitLimitNs);
         const JRec *S = tiles + b * U;
         const int tb = jb + t * T;
         bool chk = true;
@@ -641,10 +711,27 @@ __device__ __forceinline__ void process_task(const ForceParams &p, int itile_idx
             consume_tile<K, R, JL, true, NB, IDENT, V>(st, S, kbase, per, tb, p);
         else
             consume_tile<K, R, JL, false, NB, IDENT, V>(st, S, kbase, per, tb, p);
-        __syncthreads();
+        // The barrier that frees the tile buffer for the next copy also makes
+        // a timed-out wait (on any thread) the whole CTA's decision.
+        if (__syncthreads_or(!arrived)) {
+            ok = false;
+            break;
+        }
     }
     gt = g0 + ntiles;
-    if (!ok) atomicOr(p.status, ST_TMA_TIMEOUT);
+    if (!ok) {
+        // A tile copy did not arrive within its bound: no further copy is
+        // issued and the remaining tiles are skipped.  Before the epilogue
+        // reuses the tile area, wait (bounded again) for this CTA's copies
+        // still in flight -- tile t and, when it was issued, tile t + 1.
+        if (threadIdx.x == 0) {
+            const int gg = g0 + t;
+            mbar_wait_bounded(&bars[gg & 1], (gg >> 1) & 1, kWaitLimitNs);
+            if (t + 1 < ntiles) mbar_wait_bounded(&bars[(gg + 1) & 1], ((gg + 1) >> 1) & 1, kWaitLimitNs);
+            atomicOr(p.status, ST_TMA_TIMEOUT);
+        }
+        __syncthreads();
+    }
 
     // ---- epilogue: lanes -> warps -> (output | split partial)
     Partial q[R];
@@ -671,13 +758,13 @@ __device__ __forceinline__ void process_task(const ForceParams &p, int itile_idx
         for (int r = 0; r < R; ++r) {
             const int i = i0 + r * IL;
             if (i >= p.ni) continue;
-            if (p.nsplit == 1)
+            if (p.nsplit == 1 && !p.keep_partials)
                 write_final(p, i, q[r]);
             else
                 p.part[(size_t)split * p.ni + i] = q[r];
         }
     }
-    if (p.nsplit > 1 && p.tile_counter) {
+    if (p.nsplit > 1 && p.tile_counter && !p.keep_partials) {
         // Last CTA of this i-tile folds the splits (threadfence reduction).
         __shared__ int s_last;
         __threadfence();
@@ -707,6 +794,7 @@ __device__ __forceinline__ void process_task(const ForceParams &p, int itile_idx
             if (threadIdx.x == 0) p.tile_counter[itile_idx] = 0;
         }
     }
+    return ok;
 }
 
 __device__ __forceinline__ void init_bars(unsigned char *smem) {
@@ -755,18 +843,23 @@ __global__ void __launch_bounds__(256, MinBlocks<K, R>::value) batch_force_kerne
         const ForceParams p = a.items[lo];
         const int local = task - a.task0[lo];
         const int il = batch_il(p.ni);  // the item's lane shape (its H is in p.H)
+        bool ok;
         if (il == 32) {
             const int n_itiles = (p.ni + itile - 1) / itile;
-            process_task<K, IL, R, NB, IDENT, V>(p, local % n_itiles, local / n_itiles, smem, gt);
+            ok = process_task<K, IL, R, NB, IDENT, V>(p, local % n_itiles, local / n_itiles, smem, gt);
         } else if (il == 8) {
             const int it8 = (blockDim.x >> 5) / p.H * 8;
             const int n_itiles = (p.ni + it8 - 1) / it8;
-            process_task<K, 8, 1, NB, IDENT, V>(p, local % n_itiles, local / n_itiles, smem, gt);
+            ok = process_task<K, 8, 1, NB, IDENT, V>(p, local % n_itiles, local / n_itiles, smem, gt);
         } else {
             const int it1 = (blockDim.x >> 5) / p.H;
             const int n_itiles = (p.ni + it1 - 1) / it1;
-            process_task<K, 1, 1, NB, IDENT, V>(p, local % n_itiles, local / n_itiles, smem, gt);
+            ok = process_task<K, 1, 1, NB, IDENT, V>(p, local % n_itiles, local / n_itiles, smem, gt);
         }
+        // After a timed-out copy wait this CTA's barrier phases no longer
+        // match its tile count: it takes no further task (the status word
+        // already reports the failure; the other CTAs finish the list).
+        if (!ok) break;
     }
 }
 
@@ -830,6 +923,15 @@ static KernelFn pick_g4(int il, int r, bool nb) {
     return nb ? force_kernel<K, 1, 1, true, false, V> : force_kernel<K, 1, 1, false, false, V>;
 }
 
+// Potential only (energy sweeps): one i per thread, no neighbour lists.
+template <int K>
+static KernelFn pick_pot(int il, bool ident) {
+    constexpr int V = kVarUnroll4 | kVarPot;
+    if (il == 32) return ident ? force_kernel<K, 32, 1, false, true, V> : force_kernel<K, 32, 1, false, false, V>;
+    if (il == 8) return ident ? force_kernel<K, 8, 1, false, true, V> : force_kernel<K, 8, 1, false, false, V>;
+    return ident ? force_kernel<K, 1, 1, false, true, V> : force_kernel<K, 1, 1, false, false, V>;
+}
+
 static KernelFn pick(int kmode, int il, int r, bool nb, bool ident) {
     if (kmode == kKernMixedP) return pick2<kKernMixedP>(il, r, nb, ident);
     if (kmode == kKernMixedDS) return pick2<kKernMixedDS>(il, r, nb, ident);
@@ -845,6 +947,11 @@ static size_t smem_bytes(int kmode, const ForceConfig &c) {
 
 size_t partial_bytes(const ForceConfig &cfg, int ni) {
     return cfg.nsplit > 1 ? (size_t)cfg.nsplit * ni * sizeof(Partial) : 0;
+}
+
+size_t partial_bytes_fixed(int jper, int nj_pad, int ni) {
+    const int nsplit = std::max(1, (nj_pad + jper - 1) / jper);
+    return (size_t)nsplit * ni * sizeof(Partial);
 }
 
 ForceConfig choose_config(int kmode, int ni, int nj_pad, int num_sms, bool nb) {
@@ -952,12 +1059,17 @@ cudaError_t launch_force_batch(cudaStream_t s, int kmode, const ForceConfig &cfg
 }
 
 cudaError_t launch_force(cudaStream_t s, int kmode, const ForceConfig &cfg, ForceParams p,
-                         bool ident, bool nb, bool g4) {
+                         bool ident, bool nb, bool g4, bool pot) {
     if (g4 && (kmode != kKernF64 || !p.ieps2)) return cudaErrorInvalidValue;
+    if (pot && (g4 || nb || cfg.r != 1 || kmode == kKernMixedDS)) return cudaErrorInvalidValue;
     const int T = tile_size(kmode);
     const int ntiles = p.nj_pad / T;
     if (p.ni <= 0) return cudaSuccess;
-    if (ntiles <= 0) {
+    if (cfg.jper > 0) {
+        if (cfg.jper % T) return cudaErrorInvalidValue;
+        p.jper = cfg.jper;
+        p.nsplit = std::max(1, (p.nj_pad + cfg.jper - 1) / cfg.jper);
+    } else if (ntiles <= 0) {
         p.jper = T;
         p.nsplit = 1;
     } else {
@@ -970,12 +1082,13 @@ cudaError_t launch_force(cudaStream_t s, int kmode, const ForceConfig &cfg, Forc
     const int itile = G * cfg.il * cfg.r;
     dim3 grid((p.ni + itile - 1) / itile, p.nsplit);
     dim3 block(32 * cfg.warps);
-    KernelFn fn = g4 ? pick_g4(cfg.il, cfg.r, nb) : pick(kmode, cfg.il, cfg.r, nb, ident);
+    KernelFn fn = pot ? (kmode == kKernF64 ? pick_pot<kKernF64>(cfg.il, ident) : pick_pot<kKernMixedP>(cfg.il, ident))
+                      : g4 ? pick_g4(cfg.il, cfg.r, nb) : pick(kmode, cfg.il, cfg.r, nb, ident);
     size_t sm = smem_bytes(kmode, cfg);
     fn<<<grid, block, sm, s>>>(p);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
-    if (p.nsplit > 1 && !p.tile_counter) {
+    if (p.nsplit > 1 && !p.tile_counter && !p.keep_partials) {
         reduce_partials_kernel<<<(p.ni + 255) / 256, 256, 0, s>>>(p);
         e = cudaGetLastError();
     }

@@ -66,6 +66,9 @@ struct ForceParams {
     // with r2 == 0 contribute nothing (no exclusion by index), and the
     // neighbour test is r2 < h2_i on the softened r2.
     const double *ieps2;
+    // 1: every split's partial sums stay in part[split][i] (also for one
+    // split) and are not folded: the multi-GPU j-split combines them.
+    int keep_partials;
 };
 
 // A batch of calls for the persistent multi-item kernel (device pointers).
@@ -85,6 +88,7 @@ struct ForceConfig {
     int warps;    // warps per CTA
     int H;        // j-subranges per CTA
     int nsplit;   // CTAs along j
+    int jper = 0; // > 0: j per split fixed (a multiple of the tile); nsplit follows
 };
 
 void launch_scatter(cudaStream_t s, int n, const int *addr, const int *index, const double *vals,
@@ -124,15 +128,29 @@ void launch_predict(cudaStream_t s, int kmode, const double *jraw, const int *ji
 void launch_irec_from_j(cudaStream_t s, const double *jraw, const int *jindex, int cap, int i0, int ni,
                         double ti, IRec *out);
 
+// Energies of a sweep over the stored particles [i0, i0 + ni): epot =
+// 1/2 sum m_i pot_i and ekin = 1/2 sum m_i |v_i|^2 with v the i-records'
+// (predicted) velocities, masses from the raw j-state; FP64 in a fixed
+// order (kEnergyBlocks block partials, then one block).  work holds
+// 2 * kEnergyBlocks + 2 doubles; the totals land in work[2 kEnergyBlocks],
+// work[2 kEnergyBlocks + 1].
+constexpr int kEnergyBlocks = 296;
+void launch_energy(cudaStream_t s, int ni, int i0, const IRec *irec, const double *jraw, int cap,
+                   const double *pot, double *work);
+
 // kmode: kKernF64 / kKernMixedDS / kKernMixedP.
 int tile_size(int kmode);
 size_t jrec_bytes(int kmode);
 // Choose a launch configuration for ni x nj (heuristic; autotuner overrides).
 ForceConfig choose_config(int kmode, int ni, int nj_pad, int num_sms, bool nb);
-// Launch force (+ split reduction).  Returns a cudaError_t.
+// Launch force (+ split reduction).  Returns a cudaError_t.  pot: the
+// potential only (acc, jerk written as zero, nn as 0); paired mixed or FP64
+// layout, cfg.r == 1, no neighbour lists.
 cudaError_t launch_force(cudaStream_t s, int kmode, const ForceConfig &cfg, ForceParams p,
-                         bool ident, bool nb, bool g4 = false);
+                         bool ident, bool nb, bool g4 = false, bool pot = false);
 size_t partial_bytes(const ForceConfig &cfg, int ni);
+// Partial-sum bytes of a launch whose splits hold jper j each (keep_partials).
+size_t partial_bytes_fixed(int jper, int nj_pad, int ni);
 
 // Batched launches.  batch_plan fills jper/nsplit/H of one item from its own
 // (ni, nj) only -- never from the rest of the batch -- so an item's sums are
@@ -209,6 +227,17 @@ int batch_ctas(int kmode, const ForceConfig &cfg, int num_sms);
 // Self-test of the bounded copy wait: a wait on a barrier nothing arrives
 // at, which sets ST_TMA_TIMEOUT in *status after limit_ns.
 void launch_copy_wait_selftest(cudaStream_t s, unsigned *status, unsigned long long limit_ns);
+
+// Multi-GPU j-split (split.cu): order-independent fixed-point combination
+// of per-block partial sums across ranks.  agree [8 ni], sums [7 ni] and
+// negj [ni] are int64 device buffers the caller's collectives reduce.
+int split_log2_blocks(long long nblocks);
+void launch_split_agree(cudaStream_t s, int ni, int nsplit, const Partial *part, long long *agree);
+void launch_split_fix(cudaStream_t s, int ni, int nsplit, int g, long long j_offset, const Partial *part,
+                      const long long *agree, long long *sums, long long *negj);
+void launch_split_finish(cudaStream_t s, int ni, int g, long long nj_total, const long long *agree,
+                         const long long *sums, const long long *negj, double *acc, double *jerk, double *pot,
+                         int *nn);
 
 // Neighbour lists: per-i sort + compaction into ascending address order.
 // offsets[ni+1] (exclusive scan of min(count, cap)), out[total].

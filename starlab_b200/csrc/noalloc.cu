@@ -71,8 +71,9 @@ __global__ void __launch_bounds__(kTile) noalloc_force_kernel(
     double x0 = 0, y0 = 0, z0 = 0, u0 = 0, v0 = 0, w0 = 0;
     int self = -1;
     if (valid) {
-        x0 = xi[3 * i]; y0 = xi[3 * i + 1]; z0 = xi[3 * i + 2];
-        u0 = vi[3 * i]; v0 = vi[3 * i + 1]; w0 = vi[3 * i + 2];
+        const size_t b = 3 * (size_t)i;
+        x0 = xi[b]; y0 = xi[b + 1]; z0 = xi[b + 2];
+        u0 = vi[b]; v0 = vi[b + 1]; w0 = vi[b + 2];
         self = index_i ? index_i[i] : -1;
     }
     double ax = 0, ay = 0, az = 0, jx = 0, jy = 0, jz = 0, p = 0;
@@ -86,12 +87,13 @@ __global__ void __launch_bounds__(kTile) noalloc_force_kernel(
         __syncthreads();
         if (threadIdx.x < cnt) {
             const int j = tb + threadIdx.x;
-            sx[threadIdx.x] = xj[3 * j];
-            sy[threadIdx.x] = xj[3 * j + 1];
-            sz[threadIdx.x] = xj[3 * j + 2];
-            svx[threadIdx.x] = vj[3 * j];
-            svy[threadIdx.x] = vj[3 * j + 1];
-            svz[threadIdx.x] = vj[3 * j + 2];
+            const size_t b = 3 * (size_t)j;  // 3 j overflows int beyond 7e8 j
+            sx[threadIdx.x] = xj[b];
+            sy[threadIdx.x] = xj[b + 1];
+            sz[threadIdx.x] = xj[b + 2];
+            svx[threadIdx.x] = vj[b];
+            svy[threadIdx.x] = vj[b + 1];
+            svz[threadIdx.x] = vj[b + 2];
             sm[threadIdx.x] = mj[j];
         }
         __syncthreads();
@@ -119,8 +121,9 @@ __global__ void __launch_bounds__(kTile) noalloc_force_kernel(
     }
     if (!valid) return;
     if (nsplit == 1) {
-        acc[3 * i] = ax; acc[3 * i + 1] = ay; acc[3 * i + 2] = az;
-        jerk[3 * i] = jx; jerk[3 * i + 1] = jy; jerk[3 * i + 2] = jz;
+        const size_t b = 3 * (size_t)i;
+        acc[b] = ax; acc[b + 1] = ay; acc[b + 2] = az;
+        jerk[b] = jx; jerk[b + 1] = jy; jerk[b + 2] = jz;
         pot[i] = p;
         nn[i] = bj < 0 ? 0 : bj;
         return;
@@ -154,8 +157,8 @@ __global__ void noalloc_reduce_kernel(int ni, int nsplit, const NAPartial *__res
         na_take_min(a.nn_r2, a.nn_j, b.nn_r2, b.nn_j);
     }
     for (int c = 0; c < 3; ++c) {
-        acc[3 * i + c] = a.acc[c];
-        jerk[3 * i + c] = a.jerk[c];
+        acc[3 * (size_t)i + c] = a.acc[c];
+        jerk[3 * (size_t)i + c] = a.jerk[c];
     }
     pot[i] = a.pot;
     nn[i] = a.nn_j < 0 ? 0 : a.nn_j;
@@ -210,6 +213,13 @@ extern "C" int g6b200_force_noalloc(int nj, const double *xj, const double *vj, 
     DeviceSetup *d = nullptr;
     int rc = setup_device(dev, &d);
     if (rc) return rc;
+    // A CUDA error left pending by earlier work on this thread (the caller's
+    // own or another library's) would be read back below as if this launch
+    // had failed: report it as what it is and launch nothing.
+    const cudaError_t pending = cudaPeekAtLastError();
+    if (pending != cudaSuccess)
+        return fail(-3, "g6b200_force_noalloc: a CUDA error from earlier work was pending before this call "
+                        "(%lld: see cudaGetErrorString); nothing launched", (long long)pending);
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     const int iblocks = (ni + kTile - 1) / kTile;
     const int jtiles = nj > 0 ? (nj + kTile - 1) / kTile : 1;

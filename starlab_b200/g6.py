@@ -77,6 +77,8 @@ def load_library(path=None):
         "g6b200_set_j_particles": (I, [I, I, P, P, P, P, P, P, P, P, P]),
         "g6b200_get_stats": (I, [I, ctypes.POINTER(Stats)]),
         "g6b200_sweep": (I, [I, I, I, I, D, P, P, P, P]),
+        "g6b200_calc_pot": (I, [I, I, I, P, P, D, P]),
+        "g6b200_energies": (I, [I, I, D, DP, DP, P]),
         "g6b200_last_error": (ctypes.c_char_p, []),
     }
     for name, (res, args) in sig.items():
@@ -274,6 +276,32 @@ class G6Engine:
         if rc:
             self._err("g6b200_sweep", rc)
         return (acc, jerk, pot, nn) if copy_out else None
+
+    def potential(self, nj, index, xi, eps2):
+        """Potential only (g6b200_calc_pot), chunked by npipes: pot[ni] of
+        the i-particles from the j-memory predicted to the current ti."""
+        index = np.ascontiguousarray(index, dtype=np.int32)
+        ni = index.shape[0]
+        xi = _vec(xi, ni)
+        pot = np.empty(ni)
+        npipes = self.npipes()
+        for s in range(0, ni, npipes):
+            e = min(ni, s + npipes)
+            rc = self.lib.g6b200_calc_pot(self.cid, int(nj), e - s, _ptr(index[s:e]),
+                                          _ptr(np.ascontiguousarray(xi[s:e])), float(eps2), _ptr(pot[s:e]))
+            if rc:
+                self._err("g6b200_calc_pot", rc)
+        return pot
+
+    def energies(self, nj, eps2, want_pot=False):
+        """g6b200_energies: (epot, ekin[, pot]) of the stored particles
+        [0, nj) among themselves at the current ti."""
+        ep, ek = ctypes.c_double(0), ctypes.c_double(0)
+        pot = np.empty(nj) if want_pot else None
+        rc = self.lib.g6b200_energies(self.cid, int(nj), float(eps2), ctypes.byref(ep), ctypes.byref(ek), _ptr(pot))
+        if rc:
+            self._err("g6b200_energies", rc)
+        return (ep.value, ek.value, pot) if want_pot else (ep.value, ek.value)
 
     # -- neighbour lists -----------------------------------------------
     def read_neighbour_list(self):

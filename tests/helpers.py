@@ -27,6 +27,40 @@ def snapshot(n, seed, masses=None, a_scale=1.0):
     return m, x, v, a, j
 
 
+def oracle_forces(m, x, v, eps2, threads=None):
+    """acc, jerk, pot, nn of every particle of (m, x, v) on itself from the
+    FP64 oracle (oracle/g6_oracle.c), i split over host threads (the ctypes
+    call releases the interpreter lock, so the chunks run in parallel)."""
+    import concurrent.futures as cf
+    import os
+    from oracle.oracle import G6Oracle
+    o = G6Oracle()
+    n = len(m)
+    nt = max(1, min(threads or os.cpu_count() or 1, 64))
+    edges = np.linspace(0, n, 4 * nt + 1).astype(int)
+    acc, jerk, pot = np.empty((n, 3)), np.empty((n, 3)), np.empty(n)
+    nn = np.empty(n, dtype=np.int32)
+
+    def chunk(k):
+        i0, i1 = edges[k], edges[k + 1]
+        idx = np.arange(i0, i1, dtype=np.int32)
+        a, j, p, q, _ = o.force(x, v, m, idx, x[i0:i1], v[i0:i1], eps2)
+        acc[i0:i1], jerk[i0:i1], pot[i0:i1], nn[i0:i1] = a, j, p, q
+
+    with cf.ThreadPoolExecutor(nt) as ex:
+        list(ex.map(chunk, range(len(edges) - 1)))
+    return acc, jerk, pot, nn
+
+
+def force_snapshot(n, seed, eps2, masses=None):
+    """Plummer snapshot whose acc and jerk come from one FP64 oracle force
+    evaluation of the snapshot itself (t_last = 0): the state a Hermite
+    integrator holds after its initial force call."""
+    m, x, v = ics.plummer(n, seed, masses=masses)
+    a, j, _, _ = oracle_forces(m, x, v, eps2)
+    return m, x, v, a, j
+
+
 def near_tie_mask(xj, xi_list, nn_ref, rel=1e-6, index_i=None):
     """True where the nearest neighbour is ambiguous: the second-nearest r^2
     lies within `rel` of the nearest."""

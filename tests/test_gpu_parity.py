@@ -16,7 +16,7 @@ FP64 oracle):
 import numpy as np
 import pytest
 
-from helpers import near_tie_mask, rel_err, rel_err_vec, snapshot
+from helpers import force_snapshot, near_tie_mask, rel_err, rel_err_vec, snapshot
 
 pytestmark = pytest.mark.gpu
 
@@ -36,8 +36,11 @@ def new_engine(mode, npipes=65536):
 
 @pytest.fixture(scope="module")
 def c2(oracle):
+    """The single-call sweep configuration: N_j = 65536 Plummer snapshot
+    whose acc and jerk come from one FP64 oracle force evaluation (t_last =
+    0), predicted to the block time TI."""
     n = 65536
-    m, x, v, a, j = snapshot(n, 7)
+    m, x, v, a, j = force_snapshot(n, 7, EPS2)
     xp, vp = oracle.predict(TI, 0.0, x, v, 0.5 * a, j / 6.0)
     return dict(n=n, m=m, x=x, v=v, a=a, j=j, xp=xp, vp=vp)
 

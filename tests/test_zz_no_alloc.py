@@ -76,3 +76,63 @@ def test_noalloc_rejects_sizes_beyond_the_static_array():
     rc = f(10, None, None, None, limit + 1, None, None, None, 1e-6, None, None, None, None, None)
     assert rc == -1
     assert b"scratch limit" in lib.g6b200_last_error()
+
+
+def test_noalloc_direct_path_no_index_and_empty_j():
+    """The remaining branches, each against the engine's FP64 mode: ni at
+    the limit (one j-split, results written directly, the whole array's
+    bound), no index_i (no pair skipped: the engine with indices that match
+    no j), and nj = 0 (zero forces, nn = 0)."""
+    import torch
+    from starlab_b200 import G6Engine, ics
+
+    torch.cuda.set_device(0)
+    lib, f = _fn()
+    limit = 32768  # G6B200_NOALLOC_MAX_NI
+    n, eps2 = 20000, 1e-6
+    m, x, v = ics.plummer(n, 2718)
+    z = np.zeros((n, 3))
+    eng = G6Engine(cluster_id=778, precision="fp64", npipes=limit)
+    eng.set_j_particles(0.0, m, z, z, v, x)
+    eng.set_ti(0.0)
+
+    def dev(a, dtype=torch.float64):
+        return torch.from_numpy(np.ascontiguousarray(a)).to(device="cuda", dtype=dtype)
+
+    def call(nj, xj, vj, mj, ni, ii, xi, vi):
+        out = (torch.empty((ni, 3), dtype=torch.float64, device="cuda"),
+               torch.empty((ni, 3), dtype=torch.float64, device="cuda"),
+               torch.empty(ni, dtype=torch.float64, device="cuda"),
+               torch.empty(ni, dtype=torch.int32, device="cuda"))
+        ptr = lambda t: None if t is None else t.data_ptr()  # noqa: E731
+        rc = f(nj, ptr(xj), ptr(vj), ptr(mj), ni, ptr(ii), xi.data_ptr(), vi.data_ptr(), eps2,
+               *[o.data_ptr() for o in out], None)
+        assert rc == 0, lib.g6b200_last_error()
+        torch.cuda.synchronize()
+        return tuple(o.cpu().numpy() for o in out)
+
+    def close(got, want):
+        ea = np.linalg.norm(got[0] - want[0], axis=1) / np.linalg.norm(want[0], axis=1)
+        ej = np.linalg.norm(got[1] - want[1], axis=1) / np.linalg.norm(want[1], axis=1)
+        ep = np.abs(got[2] - want[2]) / np.abs(want[2])
+        assert ea.max() <= TOL and ej.max() <= TOL and ep.max() <= TOL, (ea.max(), ej.max(), ep.max())
+        assert np.array_equal(got[3], want[3])
+
+    xj, vj, mj = dev(x), dev(v), dev(m)
+    # ni at the limit: points near the cluster's own particles, each with
+    # the index of the particle it sits next to (that pair is skipped)
+    rng = np.random.default_rng(3)
+    sel = rng.integers(0, n, limit)
+    xq = x[sel] + rng.normal(scale=1e-3, size=(limit, 3))
+    vq = v[sel]
+    idx = sel.astype(np.int32)
+    want = eng.force(n, idx, xq, vq, eps2)
+    close(call(n, xj, vj, mj, limit, dev(idx, torch.int32), dev(xq), dev(vq)), want)
+    # no index_i: nothing skipped, as the engine with an index no j carries
+    ni = 500
+    want = eng.force(n, np.full(ni, -1, dtype=np.int32), xq[:ni], vq[:ni], eps2)
+    close(call(n, xj, vj, mj, ni, None, dev(xq[:ni]), dev(vq[:ni])), want)
+    # nj = 0: no j, zero sums, nn = 0
+    acc, jerk, pot, nn = call(0, None, None, None, 64, None, dev(xq[:64]), dev(vq[:64]))
+    assert not acc.any() and not jerk.any() and not pot.any() and not nn.any()
+    eng.close()
