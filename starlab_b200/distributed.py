@@ -4,116 +4,170 @@ The reference's only distributed scheme (kira_ev.C:275-420, under -DUSEMPI)
 gives every rank a contiguous range of the top-level nodes as j-particles,
 computes each i's partial acc/jerk/pot over that range, and combines them
 with MPI_Allreduce: SUM for the sums (kira_ev.C:327-328) and MINLOC for the
-nearest neighbour (kira_ev.C:409-410).  SplitCluster does the same with
-one engine per rank and torch.distributed (NCCL over NVLink on GPUs, gloo
-on CPU):
+nearest neighbour (kira_ev.C:409-410).
 
-  * rank r holds j-addresses [off_r, off_r + n_r) at local addresses
+SplitCluster keeps the whole exchange on the device and makes it
+independent of the rank count:
+
+  * the global j-set is cut into blocks of `block_j` j; rank r holds a
+    contiguous run of whole blocks (`block_range`) at local addresses
     0..n_r-1 (index == address, so the engine's fast self test applies);
-  * a force call evaluates the i-block against the local slice (an i
-    outside the slice gets an index no local j has);
-  * acc, jerk and pot (FP64) are summed over ranks with one all_reduce;
-  * each rank's nearest-neighbour candidate is scored by its r^2 (FP64, the
-    j predicted to the block time), candidates are all-gathered and every
-    rank keeps the smallest (r^2, global address) -- first address on ties,
-    as update_nn_coll (hdyn_inline.C:44) does.
+  * a force call computes, per block, the FP64 partial sums of the i-block
+    (one split of the force kernel, computed identically on whichever rank
+    holds the block) -- g6b200_split_begin, which also writes each (i,
+    quantity)'s largest exponent and each i's smallest nearest-neighbour r^2;
+  * all_reduce MAX of those (int64): every rank now has the same fixed-point
+    scale per (i, quantity) and the global smallest r^2;
+  * g6b200_split_fix converts every block partial to 64-bit fixed point on
+    that scale and sums them exactly (int64), and proposes its smallest
+    global j whose r^2 equals the global minimum;
+  * all_reduce SUM of the fixed-point sums and MAX of the negated j (the
+    first address on ties, as update_nn_coll, hdyn_inline.C:44);
+  * g6b200_split_finish converts back to FP64.
 
-`local_force(xj, vj, mj, local_index, xi, vi, eps2)` may replace the GPU
-engine for the per-rank partial sums (used on machines without a GPU to
-test the exchange).
+Integer sums are exact and order-independent, so the results are
+bit-identical for any number of ranks (given the same block size).  All
+collectives are on int64 device tensors (NCCL over NVLink on GPUs; gloo on
+CPU for the tests); no host round trip.
+
+The per-rank work is behind a small backend interface (begin / fix /
+finish on torch tensors), `EngineBackend` by default; tests substitute a
+CPU stand-in to exercise the exchange on machines without a GPU.
 """
+import ctypes
+
 import numpy as np
+
+BLOCK_J = 8192  # j per block (a multiple of the force kernel's tiles)
 
 
 def slice_of(n, world, rank):
-    """Contiguous j-range of a rank (the reference's decomp, kira_ev.C:135-148)."""
+    """Contiguous range of a rank (the reference's decomp, kira_ev.C:135-148)."""
     base, extra = divmod(n, world)
     off = rank * base + min(rank, extra)
     return off, base + (1 if rank < extra else 0)
 
 
+def block_range(n, block_j, world, rank):
+    """(first global address, count) of rank's run of whole blocks: the
+    blocks are dealt out contiguously, as evenly as they divide."""
+    nblocks = (n + block_j - 1) // block_j
+    b0, nb = slice_of(nblocks, world, rank)
+    off = min(n, b0 * block_j)
+    end = min(n, (b0 + nb) * block_j)
+    return off, end - off
+
+
+class EngineBackend:
+    """Per-rank work on this rank's GPU through the C ABI (libg6b200.so)."""
+
+    def __init__(self, cluster_id, precision, npipes, device):
+        import torch
+        from .g6 import G6Engine, _ptr
+        self.torch = torch
+        self.dev = torch.device(device)
+        self.eng = G6Engine(cluster_id=cluster_id, precision=precision, npipes=npipes)
+        self.lib, self.cid, self._ptr = self.eng.lib, self.eng.cid, _ptr
+        P, I, D, LL = ctypes.c_void_p, ctypes.c_int, ctypes.c_double, ctypes.c_longlong
+        for name, res, args in (
+                ("g6b200_split_begin", I, [I, I, I, P, P, P, D, I, P, P]),
+                ("g6b200_split_fix", I, [I, LL, LL, P, P, P, P]),
+                ("g6b200_split_finish", I, [I, LL, LL, P, P, P, P, P, P, P, P]),
+                ("g6b200_set_position_range", I, [I, D])):
+            f = getattr(self.lib, name)
+            f.restype, f.argtypes = res, args
+
+    def _stream(self):
+        return ctypes.c_void_p(self.torch.cuda.current_stream(self.dev).cuda_stream)
+
+    def _chk(self, what, rc):
+        if rc:
+            self.eng._err(what, rc)
+
+    def set_position_range(self, xmax):
+        self.lib.g6b200_set_position_range(self.cid, float(xmax))
+
+    def load(self, tj, m, j6, a2, v, x):
+        self.eng.set_j_particles(tj, m, j6, a2, v, x)
+
+    def begin(self, ti, nj, local_index, xi, vi, eps2, block_j):
+        ni = len(local_index)
+        self.eng.set_ti(ti)
+        agree = self.torch.empty(8 * ni, dtype=self.torch.int64, device=self.dev)
+        idx = np.ascontiguousarray(local_index, np.int32)
+        xi = np.ascontiguousarray(xi, np.float64)
+        vi = np.ascontiguousarray(vi, np.float64)
+        self._keep = (idx, xi, vi)
+        self._chk("g6b200_split_begin", self.lib.g6b200_split_begin(
+            self.cid, int(nj), ni, self._ptr(idx), self._ptr(xi), self._ptr(vi), float(eps2), int(block_j),
+            ctypes.c_void_p(agree.data_ptr()), self._stream()))
+        return agree
+
+    def fix(self, nblocks, j_offset, agree):
+        ni = agree.numel() // 8
+        sums = self.torch.empty(7 * ni, dtype=self.torch.int64, device=self.dev)
+        negj = self.torch.empty(ni, dtype=self.torch.int64, device=self.dev)
+        self._chk("g6b200_split_fix", self.lib.g6b200_split_fix(
+            self.cid, int(nblocks), int(j_offset), ctypes.c_void_p(agree.data_ptr()),
+            ctypes.c_void_p(sums.data_ptr()), ctypes.c_void_p(negj.data_ptr()), self._stream()))
+        return sums, negj
+
+    def finish(self, nblocks, n, agree, sums, negj):
+        ni = negj.numel()
+        acc, jerk, pot = np.empty((ni, 3)), np.empty((ni, 3)), np.empty(ni)
+        nn = np.empty(ni, dtype=np.int32)
+        self._chk("g6b200_split_finish", self.lib.g6b200_split_finish(
+            self.cid, int(nblocks), int(n), ctypes.c_void_p(agree.data_ptr()), ctypes.c_void_p(sums.data_ptr()),
+            ctypes.c_void_p(negj.data_ptr()), self._stream(), self._ptr(acc), self._ptr(jerk), self._ptr(pot),
+            self._ptr(nn)))
+        return acc, jerk, pot, nn
+
+    def close(self):
+        self.eng.close()
+
+
 class SplitCluster:
-    def __init__(self, dist, n, precision="fp64", cluster_id=900, local_force=None, device="cpu"):
+    def __init__(self, dist, n, precision="fp64", cluster_id=900, block_j=BLOCK_J, backend=None, device=None):
         self.d = dist
         self.n = int(n)
-        self.off, self.nl = slice_of(self.n, dist.world, dist.rank)
-        self.local_force = local_force
-        self.device = device
-        self.eng = None
-        if local_force is None:
-            from .g6 import G6Engine
-            self.eng = G6Engine(cluster_id=cluster_id, precision=precision, npipes=max(self.n, 1))
-        self.state = None
+        self.block_j = int(block_j)
+        self.nblocks = max(1, (self.n + self.block_j - 1) // self.block_j)
+        self.off, self.nl = block_range(self.n, self.block_j, dist.world, dist.rank)
+        if backend is None:
+            device = device or ("cuda:%d" % dist.local)
+            backend = EngineBackend(cluster_id, precision, max(self.n, 1), device)
+        self.be = backend
 
     def set_j_particles(self, tj, mass, j6, a2, v, x):
-        """Global arrays in; each rank keeps (and uploads) its own slice."""
+        """Global arrays in; each rank keeps (and uploads) its own slice.
+        Every rank sets the same fixed-point range (the global |x| bound)."""
         s = slice(self.off, self.off + self.nl)
         n = self.n
         tj = np.broadcast_to(np.asarray(tj, np.float64), (n,))
-        self.state = dict(tj=np.array(tj[s]), m=np.array(mass[s]), j6=np.array(j6[s]), a2=np.array(a2[s]),
-                          v=np.array(v[s]), x=np.array(x[s]))
-        if self.eng is not None and self.nl > 0:
-            st = self.state
-            self.eng.set_j_particles(st["tj"], st["m"], st["j6"], st["a2"], st["v"], st["x"])
+        self.be.set_position_range(float(np.abs(np.asarray(x)).max()) if n else 0.0)
+        if self.nl > 0:
+            self.be.load(np.array(tj[s]), np.array(mass[s]), np.array(j6[s]), np.array(a2[s]), np.array(v[s]),
+                         np.array(x[s]))
 
-    def _predict_local(self, ti):
-        st = self.state
-        dt = (ti - st["tj"])[:, None]
-        xp = st["x"] + dt * (st["v"] + dt * (st["a2"] + dt * st["j6"]))
-        vp = st["v"] + dt * (2.0 * st["a2"] + dt * (3.0 * st["j6"]))
-        return xp, vp
+    def _all_reduce(self, t, op):
+        if self.d.world > 1:
+            self.d.dist.all_reduce(t, op=getattr(self.d.dist.ReduceOp, op))
 
     def force(self, ti, index, xi, vi, eps2):
         """acc, jerk, pot, nn (global addresses) of the i-block, on every rank."""
-        import torch
         index = np.asarray(index, np.int64)
         ni = index.shape[0]
         xi = np.ascontiguousarray(xi, np.float64).reshape(ni, 3)
         vi = np.ascontiguousarray(vi, np.float64).reshape(ni, 3)
+        # an i outside this rank's run gets an index no local j has
         local_idx = np.where((index >= self.off) & (index < self.off + self.nl), index - self.off,
                              self.nl + 1).astype(np.int32)
-        if self.nl == 0:
-            acc, jerk, pot = np.zeros((ni, 3)), np.zeros((ni, 3)), np.zeros(ni)
-            nn = np.full(ni, -1, np.int64)
-        elif self.local_force is not None:
-            xp, vp = self._predict_local(ti)
-            acc, jerk, pot, nn = self.local_force(xp, vp, self.state["m"], local_idx, xi, vi, eps2)
-            nn = np.asarray(nn, np.int64)
-        else:
-            self.eng.set_ti(ti)
-            acc, jerk, pot, nn = self.eng.force(self.nl, local_idx, xi, vi, eps2)
-            nn = np.asarray(nn, np.int64)
-        # score the local nn candidate in FP64 (excluding i itself / empty)
-        r2 = np.full(ni, np.inf)
-        gj = np.full(ni, np.iinfo(np.int64).max, np.int64)
-        if self.nl > 0:
-            xp, _ = self._predict_local(ti)
-            ok = (nn >= 0) & (nn < self.nl) & (nn != local_idx)
-            d = xp[np.clip(nn, 0, self.nl - 1)] - xi
-            r2 = np.where(ok, np.sum(d * d, axis=1), np.inf)
-            gj = np.where(ok, nn + self.off, np.iinfo(np.int64).max)
-        dev = self.device
-        sums = torch.from_numpy(np.concatenate([acc.ravel(), jerk.ravel(), pot])).to(dev)
-        if self.d.world > 1:
-            self.d.dist.all_reduce(sums, op=self.d.dist.ReduceOp.SUM)
-            cand_r2 = [torch.empty(ni, dtype=torch.float64, device=dev) for _ in range(self.d.world)]
-            cand_j = [torch.empty(ni, dtype=torch.int64, device=dev) for _ in range(self.d.world)]
-            self.d.dist.all_gather(cand_r2, torch.from_numpy(r2).to(dev))
-            self.d.dist.all_gather(cand_j, torch.from_numpy(gj).to(dev))
-            r2s = np.stack([c.cpu().numpy() for c in cand_r2])
-            js = np.stack([c.cpu().numpy() for c in cand_j])
-        else:
-            r2s, js = r2[None], gj[None]
-        sums = sums.cpu().numpy()
-        acc = sums[:3 * ni].reshape(ni, 3)
-        jerk = sums[3 * ni:6 * ni].reshape(ni, 3)
-        pot = sums[6 * ni:]
-        # lexicographic minimum over ranks of (r^2, address)
-        order = np.lexsort((js, r2s), axis=0)[0]
-        best_j = js[order, np.arange(ni)]
-        nn = np.where(best_j == np.iinfo(np.int64).max, 0, best_j).astype(np.int32)
-        return acc, jerk, pot, nn
+        agree = self.be.begin(ti, self.nl, local_idx, xi, vi, eps2, self.block_j)
+        self._all_reduce(agree, "MAX")
+        sums, negj = self.be.fix(self.nblocks, self.off, agree)
+        self._all_reduce(sums, "SUM")
+        self._all_reduce(negj, "MAX")
+        return self.be.finish(self.nblocks, self.n, agree, sums, negj)
 
     def close(self):
-        if self.eng is not None:
-            self.eng.close()
+        self.be.close()
