@@ -274,6 +274,15 @@ long long g6b200_srv_submit(g6b200_server *h, int cluster, double ti, int nj, in
  * = time from submit to completion. */
 int g6b200_srv_wait(g6b200_server *h, long long request, double (*acc)[3], double (*jerk)[3], double *pot,
                     int *nn, double *latency_s);
+/* As g6b200_srv_wait, plus the sequence number of the batch that ran the
+ * call and how many calls that batch held (the calls that shared its
+ * launch). */
+int g6b200_srv_wait_batch(g6b200_server *h, long long request, double (*acc)[3], double (*jerk)[3], double *pot,
+                          int *nn, double *latency_s, long long *batch, int *batch_size);
+/* hold != 0: the dispatchers take no new calls; hold = 0: every call
+ * pending then goes into the next batch of its lane (up to max_batch)
+ * together -- a burst gathered on purpose. */
+void g6b200_srv_hold(g6b200_server *h, int hold);
 int g6b200_srv_stats(g6b200_server *h, g6b200_srv_stats_t *out);
 void g6b200_srv_destroy(g6b200_server *h);
 

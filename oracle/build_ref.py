@@ -13,6 +13,7 @@ with g++ directly (no autotools: they are absent here), into ``oracle/_ref/``:
                        (``src/node/dyn/hdyn/stubs/grape6_stubs.c``), linked
                        last exactly as ``evolve/Makefile.am:36-48`` does;
 * tools               ``kira``, ``makeplummer``, ``makemass``, ``scale``,
+                       ``makesecondary``, ``makebinary`` (primordial binaries),
                        ``hsys_stats``, ``hscale`` (TOOLBOX mains, CPU engine);
 * ``kira_g6``/``hsys_stats_g6``  the same mains linked against
                        ``libg6b200.so`` before the stubs, i.e. the unchanged
@@ -80,6 +81,8 @@ TOOLS = {
     "hscale": "node/dyn/hdyn/util/hscale.C",
     "get_densities": "node/dyn/hdyn/util/get_densities.C",
     "compute_density": "node/dyn/util/compute_density.C",
+    "makesecondary": "node/dyn/util/makesecondary.C",
+    "makebinary": "node/dyn/init/makebinary.C",
 }
 CONFIG_H = """/* hand-written stand-in for the autoconf config.h of Starlab 4.4.4 */
 #define HAVE_LIBPTHREAD 1

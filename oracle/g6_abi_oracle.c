@@ -74,6 +74,16 @@ void g6_set_tunit_(int *u) { (void)u; }
 void g6_set_xunit_(int *u) { (void)u; }
 int g6_open_(int *id) { (void)id; return 0; }
 int g6_close_(int *id) { (void)id; return 0; }
+
+/* Calls of two i-particles sharing one index: the signature of kira's
+ * binary perturbation call (hdyn_grape6.C:3415-3587 packs both components
+ * with their top-level node's index).  Printed at exit with G6O_TRACE. */
+static long long calls_, pair_calls_;
+
+__attribute__((destructor)) static void trace_at_exit(void)
+{
+    if (getenv("G6O_TRACE")) fprintf(stderr, "g6 oracle trace: calls %lld pair_calls %lld\n", calls_, pair_calls_);
+}
 int g6_open_special(int ngpu, int *list) { (void)ngpu; (void)list; return 0; }
 int g6_open_special2(int ngpu, int *list, int nmax) { (void)ngpu; (void)list; (void)nmax; return 0; }
 int g6_reset_(int *id) { (void)id; return 0; }
@@ -104,6 +114,8 @@ void g6calc_firsthalf_(int *id, int *nj, int *ni, int index[], double xi[][3], d
     (void)id; (void)aold; (void)j6old; (void)phiold;
     nj_ = *nj;
     ni_ = *ni;
+    calls_++;
+    if (ni_ == 2 && index[0] == index[1]) pair_calls_++;
     ensure_j(nj_);
     index_ = grow(index_, 4 * (size_t)ni_);
     xi_ = grow(xi_, 24 * (size_t)ni_); vi_ = grow(vi_, 24 * (size_t)ni_); h2_ = grow(h2_, 8 * (size_t)ni_);

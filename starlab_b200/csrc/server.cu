@@ -50,6 +50,8 @@ struct Request {
     int rc = 0;
     bool done = false;
     double t_submit = 0, t_done = 0;
+    long long batch = -1;  // sequence number of the batch that ran the call
+    int batch_size = 0;    // calls in that batch
     std::condition_variable cv;  // signalled once, when done (waits on the server mutex)
 };
 
@@ -117,7 +119,17 @@ class Server {
               const double (*a2)[3], const double (*v)[3], const double (*x)[3]);
     long long submit(int c, double ti, int nj, int ni, const int *index, const double (*xi)[3],
                      const double (*vi)[3]);
-    int wait(long long id, double (*acc)[3], double (*jerk)[3], double *pot, int *nn, double *latency_s);
+    int wait(long long id, double (*acc)[3], double (*jerk)[3], double *pot, int *nn, double *latency_s,
+             long long *batch = nullptr, int *batch_size = nullptr);
+    // While held, no lane takes new calls; on release every pending call of
+    // a lane (up to max_batch) goes into its next batch together.
+    void hold(bool on) {
+        {
+            std::lock_guard<std::mutex> lk(mu_);
+            held_ = on;
+        }
+        cv_work_.notify_all();
+    }
     ServerStats stats() {
         std::lock_guard<std::mutex> lk(mu_);
         return stats_;
@@ -151,6 +163,8 @@ class Server {
     std::map<long long, std::shared_ptr<Request>> inflight_;
     long long next_id_ = 1;
     bool stop_ = false;
+    bool held_ = false;
+    long long batch_seq_ = 0;
     bool started_ = false;
     ServerStats stats_;
     std::string trace_path_;
@@ -330,7 +344,8 @@ long long Server::submit(int c, double ti, int nj, int ni, const int *index, con
     return r->id;
 }
 
-int Server::wait(long long id, double (*acc)[3], double (*jerk)[3], double *pot, int *nn, double *latency_s) {
+int Server::wait(long long id, double (*acc)[3], double (*jerk)[3], double *pot, int *nn, double *latency_s,
+                 long long *batch, int *batch_size) {
     std::shared_ptr<Request> r;
     {
         std::unique_lock<std::mutex> lk(mu_);
@@ -347,6 +362,8 @@ int Server::wait(long long id, double (*acc)[3], double (*jerk)[3], double *pot,
     if (pot) memcpy(pot, r->pot.data(), 8 * n);
     if (nn) memcpy(nn, r->nn.data(), 4 * n);
     if (latency_s) *latency_s = r->t_done - r->t_submit;
+    if (batch) *batch = r->batch;
+    if (batch_size) *batch_size = r->batch_size;
     return 0;
 }
 
@@ -356,11 +373,16 @@ void Server::loop(Lane &L) {
         std::vector<std::shared_ptr<Request>> batch;
         {
             std::unique_lock<std::mutex> lk(mu_);
-            cv_work_.wait(lk, [&] { return stop_ || !L.pending.empty(); });
+            cv_work_.wait(lk, [&] { return stop_ || (!held_ && !L.pending.empty()); });
             if (stop_ && L.pending.empty()) return;
             while (!L.pending.empty() && (int)batch.size() < max_batch_) {
                 batch.push_back(L.pending.front());
                 L.pending.pop_front();
+            }
+            const long long seq = batch_seq_++;
+            for (auto &r : batch) {
+                r->batch = seq;
+                r->batch_size = (int)batch.size();
             }
         }
         const double tb0 = now();
@@ -681,6 +703,15 @@ __attribute__((visibility("default"))) int g6b200_srv_wait(g6b200_server *h, lon
                                                            double *latency_s) {
     return h->s->wait(request, acc, jerk, pot, nn, latency_s);
 }
+
+__attribute__((visibility("default"))) int g6b200_srv_wait_batch(g6b200_server *h, long long request,
+                                                                 double (*acc)[3], double (*jerk)[3], double *pot,
+                                                                 int *nn, double *latency_s, long long *batch,
+                                                                 int *batch_size) {
+    return h->s->wait(request, acc, jerk, pot, nn, latency_s, batch, batch_size);
+}
+
+__attribute__((visibility("default"))) void g6b200_srv_hold(g6b200_server *h, int hold) { h->s->hold(hold != 0); }
 
 __attribute__((visibility("default"))) int g6b200_srv_stats(g6b200_server *h, g6b200_srv_stats_t *out) {
     g6::ServerStats st = h->s->stats();

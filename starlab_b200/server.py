@@ -31,6 +31,10 @@ def _bind(lib):
     lib.g6b200_srv_submit.restype = L
     lib.g6b200_srv_submit.argtypes = [P, I, D, I, I, P, P, P]
     lib.g6b200_srv_wait.argtypes = [P, L, P, P, P, P, ctypes.POINTER(ctypes.c_double)]
+    lib.g6b200_srv_wait_batch.argtypes = [P, L, P, P, P, P, ctypes.POINTER(ctypes.c_double),
+                                          ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_int)]
+    lib.g6b200_srv_hold.argtypes = [P, I]
+    lib.g6b200_srv_hold.restype = None
     lib.g6b200_srv_stats.argtypes = [P, ctypes.POINTER(SrvStats)]
     lib.g6b200_srv_destroy.argtypes = [P]
     lib.g6b200_srv_destroy.restype = None
@@ -88,6 +92,22 @@ class Server:
         if rc:
             raise G6Error("g6b200_srv_wait", rc, self.lib.g6b200_last_error().decode())
         return acc, jerk, pot, nn, lat.value
+
+    def wait_batch(self, rid_ni):
+        """wait() plus (batch sequence number, calls in that batch)."""
+        rid, ni = rid_ni
+        acc, jerk, pot = np.empty((ni, 3)), np.empty((ni, 3)), np.empty(ni)
+        nn = np.empty(ni, dtype=np.int32)
+        lat, b, bs = ctypes.c_double(0), ctypes.c_longlong(-1), ctypes.c_int(0)
+        rc = self.lib.g6b200_srv_wait_batch(self.h, rid, _p(acc), _p(jerk), _p(pot), _p(nn), ctypes.byref(lat),
+                                            ctypes.byref(b), ctypes.byref(bs))
+        if rc:
+            raise G6Error("g6b200_srv_wait_batch", rc, self.lib.g6b200_last_error().decode())
+        return acc, jerk, pot, nn, lat.value, b.value, bs.value
+
+    def hold(self, on=True):
+        """Gather calls without dispatching them (released by hold(False))."""
+        self.lib.g6b200_srv_hold(self.h, 1 if on else 0)
 
     def stats(self):
         st = SrvStats()

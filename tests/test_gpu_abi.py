@@ -223,3 +223,26 @@ def test_small_call_path_matches_copy_path(mode):
     assert len(outs[0]) == len(outs[1])
     for k, (r1, r2) in enumerate(zip(*outs)):
         assert same(r1, r2), k
+
+
+@pytest.mark.parametrize("mode", ["fp64", "mixed"])
+def test_lasthalf_without_nn_equals_lasthalf2(mode, oracle):
+    """g6calc_lasthalf_ (grape6.h:68-78) returns the same acc, jerk and pot
+    as g6calc_lasthalf2_ for the same call, only without the nearest
+    neighbour; both agree with the oracle."""
+    m, x, v, a, j = snapshot(4096, 12)
+    e = eng(mode, npipes=512)
+    e.set_j_particles(0.0, m, j / 6.0, 0.5 * a, v, x)
+    ti = 1.0 / 512
+    e.set_ti(ti)
+    xp, vp = oracle.predict(ti, 0.0, x, v, 0.5 * a, j / 6.0)
+    idx = np.arange(100, 612, dtype=np.int32)
+    e.calc_firsthalf(4096, idx, xp[idx], vp[idx], 1e-6)
+    a1, j1, p1 = e.calc_lasthalf()
+    e.calc_firsthalf(4096, idx, xp[idx], vp[idx], 1e-6)
+    a2, j2, p2, nn2 = e.calc_lasthalf2()
+    assert np.array_equal(a1, a2) and np.array_equal(j1, j2) and np.array_equal(p1, p2)
+    ra, rj, rp, rn, _ = oracle.force(xp, vp, m, idx, xp[idx], vp[idx], 1e-6)
+    tol = 1e-12 if mode == "fp64" else 1e-6
+    assert rel_err_vec(a1, ra).max() <= tol and rel_err(p1, rp).max() <= tol
+    e.close()

@@ -89,3 +89,73 @@ def test_kira_recovers_from_injected_engine_error(plummer1024):
                    {"G6B200_PRECISION": "fp64", "G6B200_FAULT_LASTHALF": "50"}, d)
     assert "Resetting GRAPE and retrying" in gpu
     assert len(energies(gpu)) >= 2
+
+
+def _trace(log, key):
+    m = re.search(r"g6b200\[0\] trace: .*?%s (\d+)" % key, log)
+    return int(m.group(1)) if m else None
+
+
+@pytest.fixture(scope="module")
+def binaries1024(tmp_path_factory):
+    """N = 1024 Plummer sphere (seed 42) with primordial binaries from the
+    reference's own generators: makesecondary gives 10% of the stars a
+    secondary (mass ratio >= 0.25), makebinary puts them on orbits of
+    0.5-2 kT (soft enough that some binaries' perturber lists overflow)."""
+    tools = [_need(t) for t in ("makeplummer", "makesecondary", "makebinary")]
+    d = tmp_path_factory.mktemp("kira_bin")
+    snap = os.path.join(d, "b1024.snap")
+    p1 = subprocess.Popen([tools[0], "-n", "1024", "-s", "42", "-i"], stdout=subprocess.PIPE,
+                          stderr=subprocess.DEVNULL)
+    p2 = subprocess.Popen([tools[1], "-f", "0.1", "-q", "-l", "0.25", "-s", "7"], stdin=p1.stdout,
+                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL)
+    with open(snap, "w") as f:
+        p3 = subprocess.run([tools[2], "-f", "3", "-o", "3", "-l", "0.5", "-u", "2", "-s", "9"], stdin=p2.stdout,
+                            stdout=f, stderr=subprocess.DEVNULL)
+    p1.wait(), p2.wait()
+    assert p3.returncode == 0
+    return str(d), snap
+
+
+BIN_ARGS = ["-t", "0.125", "-d", "0.0625", "-e", "0.001", "-a", "0.02"]
+
+
+def test_kira_binaries_and_perturbation_calls(binaries1024):
+    """kira's GRAPE-6 branch with binaries: the perturbation call
+    (grape6_calculate_perturbation, hdyn_grape6.C:3415-3587, issued from
+    hdyn_ev.C:3127 when a binary's perturber list overflows) sends ni = 2
+    calls with both components under one index; the engine's trace counts
+    them.  Energy error within 2x of the same kira branch over the CPU
+    GRAPE-6 oracle (kira_g6o, oracle/g6_abi_oracle.c), which counts the
+    same call shape; kira -0 (no GRAPE) is reported beside them."""
+    d, snap = binaries1024
+    gpu = run_kira(_need("kira_g6"), snap, BIN_ARGS, {"G6B200_PRECISION": "fp64", "G6B200_TRACE": "1"}, d)
+    cpu_g6 = run_kira(_need("kira_g6o"), snap, BIN_ARGS, {"G6O_TRACE": "1"}, d)
+    cpu = run_kira(_need("kira"), snap, ["-0"] + BIN_ARGS, {}, d)
+    pairs = _trace(gpu, "pair_calls")
+    m = re.search(r"g6 oracle trace: calls (\d+) pair_calls (\d+)", cpu_g6)
+    assert pairs is not None and m is not None
+    assert pairs > 0 and int(m.group(2)) > 0, (pairs, m.group(0))
+    eg, eo, ec = energies(gpu), energies(cpu_g6), energies(cpu)
+    assert eg[0] == pytest.approx(eo[0], rel=1e-12) and eg[0] == pytest.approx(ec[0], rel=1e-12)
+    de_g = max(abs(e - eg[0]) for e in eg[1:])
+    de_o = max(abs(e - eo[0]) for e in eo[1:])
+    de_c = max(abs(e - ec[0]) for e in ec[1:])
+    print("binaries: |dE| kira_g6 %.3e kira_g6o %.3e kira -0 %.3e; pair calls %d (oracle %s)"
+          % (de_g, de_o, de_c, pairs, m.group(2)))
+    assert de_g <= 2.0 * de_o, (de_g, de_o, de_c)
+
+
+def test_kira_jp_buffer_mode_identical(plummer1024):
+    """kira -2 batches j-particle writes through g6_initialize_jp_buffer_ /
+    g6_flush_jp_buffer_ (hdyn_grape6.C:266-271, :672-673).  The engine
+    stages j updates either way, so the run gives the same energies at every
+    log point as the run without -2."""
+    d, snap = plummer1024
+    args = ["-t", "0.25", "-d", "0.0625", "-e", "0.001", "-a", "0.02"]
+    plain = run_kira(_need("kira_g6"), snap, args, {"G6B200_PRECISION": "fp64"}, d)
+    dma = run_kira(_need("kira_g6"), snap, ["-2"] + args, {"G6B200_PRECISION": "fp64"}, d)
+    assert "g6_initialize_jp_buffer_" in dma
+    ep, ed = energies(plain), energies(dma)
+    assert len(ep) >= 4 and ep == ed, (ep, ed)
+

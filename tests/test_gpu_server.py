@@ -35,14 +35,21 @@ def test_alone_equals_mixed_and_matches_oracle(oracle):
     c0, (m, x, v, a, j) = ids[0]
     xp, vp = oracle.predict(ti, 0.0, x, v, 0.5 * a, j / 6.0)
     idx = np.arange(10, 300, dtype=np.int32)
-    alone = srv.wait(srv.submit(c0, ti, len(m), idx, xp[idx], vp[idx]))
-    # the same call again, now together with calls of the other clusters
+    alone = srv.wait_batch(srv.submit(c0, ti, len(m), idx, xp[idx], vp[idx]))
+    assert alone[6] == 1  # ran alone
+    # the same call again, now together with calls of the other clusters:
+    # all gathered while the dispatchers are held, then released at once
+    srv.hold(True)
     reqs = []
     for c, (mm, xx, vv, aa, jj) in ids[1:]:
         xq, vq = oracle.predict(ti, 0.0, xx, vv, 0.5 * aa, jj / 6.0)
         k = np.arange(0, len(mm), 3, dtype=np.int32)
         reqs.append((srv.submit(c, ti, len(mm), k, xq[k], vq[k]), c, k, xq, vq, mm))
-    mixed = srv.wait(srv.submit(c0, ti, len(m), idx, xp[idx], vp[idx]))
+    rmix = srv.submit(c0, ti, len(m), idx, xp[idx], vp[idx])
+    srv.hold(False)
+    mixed = srv.wait_batch(rmix)
+    # the mixed call shared its launch with the other clusters' calls
+    assert mixed[6] == 1 + len(reqs), mixed[5:]
     for q in range(4):
         assert np.array_equal(alone[q], mixed[q])
     ra, rj, rp, rn, _ = oracle.force(xp, vp, m, idx, xp[idx], vp[idx], EPS2)
@@ -50,7 +57,9 @@ def test_alone_equals_mixed_and_matches_oracle(oracle):
     assert rel_err_vec(alone[1], rj).max() < 1e-5
     assert rel_err(alone[2], rp).max() < 1e-6
     for rid, c, k, xq, vq, mm in reqs:
-        got = srv.wait(rid)
+        got = srv.wait_batch(rid)
+        assert got[5] == mixed[5]  # the same batch
+        got = got[:5]
         sub = k[::50]
         ra, rj, rp, rn, _ = oracle.force(xq, vq, mm, sub, xq[sub], vq[sub], EPS2)
         assert rel_err_vec(got[0][::50], ra).max() < 1e-6
