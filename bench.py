@@ -142,19 +142,14 @@ def measured_peaks():
 
 
 def traffic_from_profile():
-    """DRAM bytes of one full-sweep force launch (the launch `value` times)
-    from the committed ncu summary profiles/force_sweep_traffic_n262144.md
-    ('traffic_bytes_full_sweep_launch: B'); None when not captured."""
-    p = os.path.join(REPO, "profiles", "force_sweep_traffic_n262144.md")
-    if not os.path.exists(p):
+    """DRAM bytes of one full-sweep force launch (the launch `value` times),
+    from one ncu capture kept in profiles/force_sweep_traffic_n262144.json;
+    None when not captured."""
+    p = os.path.join(REPO, "profiles", "force_sweep_traffic_n262144.json")
+    try:
+        return float(json.load(open(p))["traffic_bytes_full_sweep_launch"])
+    except (OSError, ValueError, KeyError):
         return None
-    for line in open(p):
-        if line.strip().startswith("traffic_bytes_full_sweep_launch:"):
-            try:
-                return float(line.split(":", 1)[1].split()[0])
-            except (ValueError, IndexError):
-                return None
-    return None
 
 
 # ---------------------------------------------------------------- workload
@@ -206,28 +201,36 @@ def ensemble_section(nc, t_full, seed):
     return out
 
 
-def served_section(seed):
+def served_section(seed, rates=(2000.0, 20000.0), n_calls=3000):
     """Force calls from 48 clusters (N log-uniform in [512, 65536]) arriving
-    as Poisson(2000/s), ni ~ 1/ni on [1, N]: the batching server vs the plain
-    engine serving the same stream one call at a time."""
+    as a Poisson process, ni ~ 1/ni on [1, N]: the batching server vs the
+    plain engine serving the same stream one call at a time, at the
+    configured 2000 calls/s and at a rate well above what one call at a time
+    can serve (the queue then builds and batches fill)."""
     from starlab_b200 import G6Engine
     from starlab_b200.server import Server
     from starlab_b200.stream import make_clusters, make_stream, run_served, run_sequential
     clusters = make_clusters(48, seed)
-    calls = make_stream(clusters, 2000.0, 3000, seed)
-    srv = Server(precision="mixed")
-    lat, wall, inter = run_served(srv, clusters, calls)
-    st = srv.stats()
-    srv.close()
-    lat2, wall2, inter2 = run_sequential(
-        lambda k, n: G6Engine(cluster_id=3000 + k, precision="mixed", npipes=n), clusters, calls)
-    return {"clusters": len(clusters), "calls": len(calls), "rate_per_s": 2000.0,
+    out = {"clusters": len(clusters), "calls": n_calls}
+    for rate in rates:
+        calls = make_stream(clusters, rate, n_calls, seed)
+        srv = Server(precision="mixed")
+        lat, wall, inter = run_served(srv, clusters, calls)
+        st = srv.stats()
+        srv.close()
+        lat2, wall2, inter2 = run_sequential(
+            lambda k, n: G6Engine(cluster_id=3000 + k, precision="mixed", npipes=n), clusters, calls)
+        out["rate_%d" % int(rate)] = {
+            "rate_per_s": rate,
             "served": {"p50_ms": float(np.percentile(lat, 50) * 1e3), "p99_ms": float(np.percentile(lat, 99) * 1e3),
                        "interactions_per_s": inter / wall, "batches": st["batches"],
-                       "mean_batch": st["requests"] / max(1, st["batches"]), "max_batch": st["max_batch"]},
+                       "mean_batch": st["requests"] / max(1, st["batches"]), "max_batch": st["max_batch"],
+                       "wall_s": wall},
             "one_call_at_a_time": {"p50_ms": float(np.percentile(lat2, 50) * 1e3),
                                    "p99_ms": float(np.percentile(lat2, 99) * 1e3),
-                                   "interactions_per_s": inter2 / wall2}}
+                                   "interactions_per_s": inter2 / wall2, "wall_s": wall2},
+            "served_over_plain": (inter / wall) / (inter2 / wall2)}
+    return out
 
 
 def grape4_section(seed, n=65536, sweeps=3):
@@ -319,29 +322,35 @@ def _rel(a, b):
     return np.linalg.norm(a - b, axis=1) / np.linalg.norm(b, axis=1) if a.ndim == 2 else np.abs(a - b) / np.abs(b)
 
 
-def cpu_baseline(n, seed, cores, per_core=640, gpu=None):
+def cpu_baseline(n, seed, cores, per_core=640, gpu=None, state=None):
     """Starlab's FP64 force loop on a bounded sample of i (rank 0, N=1):
-    per_core i-particles per host thread against all N j.  When `gpu` holds
-    the engine's (acc, jerk, pot, nn) for every particle of the same state
-    (t = 0, no prediction), the reference's results for the sample also score
-    them: per-particle relative error of acc, jerk and pot, nn mismatches."""
+    per_core i-particles per host thread against all N j, every particle
+    first predicted to the block time by the reference's predict_loworder.
+    `state` = (acc, jerk, ti): the j-state's acc and jerk (tj = 0) and the
+    block time of a timed step (default: zero acc and jerk, ti = 0).  When
+    `gpu` holds the engine's (acc, jerk, pot, nn) for every particle at that
+    step, the reference's results for the sample also score them:
+    per-particle relative error of acc, jerk and pot, nn mismatches."""
     m, x, v = make_cluster(n, seed)
     z = np.zeros((n, 3))
+    a0, j0, ti = state if state is not None else (z, z, 0.0)
     try:
         from oracle.oracle import RefForce
         ref = RefForce()
         ni = int(min(n, per_core * cores))
         ilist = np.linspace(0, n - 1, ni).astype(np.int32)
-        out = ref.force(m, x, v, z, z, 0.0, 0.0, float(np.sqrt(EPS2)), ilist=ilist, nthreads=cores)
+        out = ref.force(m, x, v, a0, j0, 0.0, ti, float(np.sqrt(EPS2)), ilist=ilist, nthreads=cores)
         secs = out["seconds"]
         res = {"value": ni * (n - 1) / secs, "unit": "interactions/s", "cores": cores, "kind": "reference",
                "sample": "%d i (evenly spaced) x %d j, hdyn::flat_calculate_acc_and_jerk on %d threads; "
-                         "force loop %.2f s" % (ni, n, cores, secs)}
+                         "force loop %.2f s" % (ni, n, cores, secs),
+               "sample_i": int(ni), "sample_seconds": secs}
         if gpu is not None:
             acc, jerk, pot, nn = (g[ilist] for g in gpu)
             acc_err, jerk_err, pot_err = _rel(acc, out["acc"]), _rel(jerk, out["jerk"]), _rel(pot, out["pot"])
             res["accuracy_vs_reference"] = {
-                "sample_i": int(ni), "precision": "mixed",
+                "sample_i": int(ni), "precision": "mixed", "ti": ti,
+                "step": "the last timed step: j predicted from tj = 0 to ti with the step's acc/2 and jerk/6",
                 "acc": {"median": float(np.median(acc_err)), "max": float(acc_err.max())},
                 "jerk": {"median": float(np.median(jerk_err)), "max": float(jerk_err.max())},
                 "pot": {"median": float(np.median(pot_err)), "max": float(pot_err.max())},
@@ -356,7 +365,29 @@ def cpu_baseline(n, seed, cores, per_core=640, gpu=None):
         o.force(x, v, m, idx, x[:ni], v[:ni], EPS2)
         secs = time.perf_counter() - t0
         return {"value": ni * (n - 1) / secs, "unit": "interactions/s", "cores": 1, "kind": "port",
-                "sample": "%d i x %d j, oracle C restatement, 1 thread" % (ni, n)}
+                "sample": "%d i x %d j, oracle C restatement, 1 thread" % (ni, n),
+                "sample_i": ni, "sample_seconds": secs}
+
+
+def accuracy_vs_fp64(m, x, v, acc, jerk, ti, got):
+    """Every particle of the timed step (mixed) against the engine's FP64
+    mode on the same state (FP64 prediction, pair sums and accumulation;
+    pinned to <= 1e-12 of the FP64 oracle by the parity tests): per-quantity
+    median / 99.9th percentile / max relative error over all i."""
+    from starlab_b200 import G6Engine
+    n = len(m)
+    e64 = G6Engine(cluster_id=7, precision="fp64", npipes=n)
+    e64.set_j_particles(0.0, m, jerk / 6.0, 0.5 * acc, v, x)
+    e64.set_ti(ti)
+    ref = e64.sweep(n, eps2=EPS2)
+    e64.close()
+    out = {"all_i": int(n), "ti": ti, "precision": "mixed vs fp64 engine"}
+    for k, g, r, tol in (("acc", got[0], ref[0], 1e-6), ("jerk", got[1], ref[1], 1e-5), ("pot", got[2], ref[2], 1e-6)):
+        e = _rel(g, r)
+        out[k] = {"median": float(np.median(e)), "p999": float(np.quantile(e, 0.999)), "max": float(e.max()),
+                  "over_tolerance": int((e > tol).sum()), "tolerance": tol}
+    out["nn_mismatch"] = int(np.sum(got[3] != ref[3]))
+    return out
 
 
 def run_reference(args, dist):
@@ -365,17 +396,25 @@ def run_reference(args, dist):
         return
     cores = os.cpu_count() or 1
     n = args.n
-    vals = []
+    vals, secs = [], []
     last = None
     for k in range(args.warmup + args.steps):
         r = cpu_baseline(n, 11, cores, per_core=96)
         if k >= args.warmup:
             vals.append(r["value"])
+            secs.append(r.get("sample_seconds", 0.0))
         last = r
     value = statistics.median(vals)
-    per_step_ms = n * (n - 1) / value * 1e3
+    # A step is one bounded sample (sample_i i against all N j): ms_per_step
+    # is its measured time; the full sweep's time is extrapolated from the
+    # rate and labelled as such.
+    per_step_ms = statistics.median(secs) * 1e3
     line = {"metric": METRIC, "impl": "reference", "value": value, "unit": "interactions/s",
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": per_step_ms,
+            "step": "sample of %d i x %d j (of the %d-i sweep)" % (last["sample_i"], n, n),
+            "extrapolated": {"full_sweep_ms": n * (n - 1) / value * 1e3, "from_sample_i": last["sample_i"],
+                             "note": "the full 262144 x 262143 sweep on the CPU is extrapolated linearly "
+                                     "from the sample rate, not run"},
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic", "config": config_of(args, n),
             "cpu_baseline": {"value": value, "unit": "interactions/s", "cores": last["cores"], "kind": last["kind"],
@@ -393,7 +432,161 @@ def config_of(args, n):
                   "memory every step"}
 
 
+# ---------------------------------------------------------------- sub-modes
+# Bounded workloads to run under a profiler (ncu) with one command line, and
+# the energy-drift measurement:
+#   python bench.py profile-case --n 262144 --ni 16384 --mode mixed --calls 3
+#   python bench.py profile-ensemble --t 0.015625
+#   python bench.py profile-story --n 262144 --reps 3
+#   python bench.py energy-drift --n 262144 --t 1
+def profile_case(argv):
+    """A few force calls of one shape through the C ABI: an N-particle
+    Plummer/Salpeter cluster in j-memory, then `calls` firsthalf/lasthalf2
+    pairs of ni i-particles at new block times (every call runs the predictor
+    and the force kernel); prints the engine's device times per call."""
+    ap = argparse.ArgumentParser(prog="bench.py profile-case")
+    ap.add_argument("--n", type=int, default=262144)
+    ap.add_argument("--ni", type=int, default=16384)
+    ap.add_argument("--mode", default="mixed", choices=["mixed", "fp64"])
+    ap.add_argument("--calls", type=int, default=3)
+    ap.add_argument("--eps2", type=float, default=1e-8)
+    ap.add_argument("--h2", type=float, default=0.0)
+    ap.add_argument("--config", default="", help="il,r,warps,h,nsplit")
+    a = ap.parse_args(argv)
+    os.environ.setdefault("G6B200_EVENT_TIMING", "1")  # per-call device times in the stats
+    from starlab_b200 import G6Engine, ics
+    m, x, v = ics.plummer(a.n, 11, masses=ics.salpeter_masses(a.n, 12))
+    z = np.zeros((a.n, 3))
+    eng = G6Engine(cluster_id=0, precision=a.mode, npipes=max(a.ni, 1))
+    if a.config:
+        eng.set_config(*[int(t) for t in a.config.split(",")])
+    eng.set_j_particles(0.0, m, z, z, v, x)
+    idx = np.arange(a.ni, dtype=np.int32)
+    h2 = None if a.h2 <= 0 else np.full(a.ni, a.h2)
+    for c in range(a.calls):
+        eng.set_ti(1e-3 * (c + 1))
+        eng.calc_firsthalf(a.n, idx, x[:a.ni], v[:a.ni], a.eps2, h2)
+        eng.calc_lasthalf2()
+        if h2 is not None:
+            eng.read_neighbour_list()
+        st = eng.stats()
+        print(json.dumps(dict(call=c, force_ms=st["last_force_ms"], predict_ms=st["last_predict_ms"],
+                              call_ms=st["last_call_ms"], config=eng.last_config(),
+                              interactions_per_s=a.ni * a.n / (st["last_force_ms"] * 1e-3))))
+    eng.close()
+    return 0
+
+
+def profile_ensemble(argv):
+    """One slice of the bench's ensemble workload (256 Plummer clusters, N
+    log-uniform in [256, 16384], seed 2024, eps^2 = (4/N)^2, eta = 0.02,
+    mixed), from t = 0 to --t; prints the run's statistics."""
+    ap = argparse.ArgumentParser(prog="bench.py profile-ensemble")
+    ap.add_argument("--clusters", type=int, default=256)
+    ap.add_argument("--seed", type=int, default=2024)
+    ap.add_argument("--t", type=float, default=1.0 / 64)
+    ap.add_argument("--tune", action="store_true")
+    a = ap.parse_args(argv)
+    from starlab_b200 import ics
+    from starlab_b200.ensemble import Ensemble
+    rng = np.random.default_rng(a.seed)
+    ns = np.exp(rng.uniform(np.log(256), np.log(16384), a.clusters)).astype(int)
+    cl = [ics.plummer(int(n), a.seed * 1000 + k) for k, n in enumerate(ns)]
+    e = Ensemble([c[0] for c in cl], [c[1] for c in cl], [c[2] for c in cl], (4.0 / ns) ** 2, eta=0.02,
+                 precision="mixed")
+    e.start()
+    st = e.run(a.t, tune=a.tune)
+    e.close()
+    st["interactions_per_s"] = st["interactions"] / st["seconds"]
+    st["us_per_iteration"] = st["seconds"] / st["iterations"] * 1e6
+    print(json.dumps(st))
+    return 0
+
+
+def profile_story(argv):
+    """A flat N-body snapshot in the reference's output format, resident in
+    device memory, parsed --reps times corrected and --reps times raw;
+    prints the median wall time of each."""
+    ap = argparse.ArgumentParser(prog="bench.py profile-story")
+    ap.add_argument("--n", type=int, default=262144)
+    ap.add_argument("--reps", type=int, default=3)
+    ap.add_argument("--seed", type=int, default=11)
+    a = ap.parse_args(argv)
+    import torch
+    from starlab_b200 import ics
+    from starlab_b200.story import StoryReader, format_story
+    m = ics.salpeter_masses(a.n, a.seed)
+    _, x, v = ics.plummer(a.n, a.seed + 1, masses=m)
+    text = format_story(m, x + 1e-3, v - 5e-4)
+    d = torch.frombuffer(bytearray(text), dtype=torch.uint8).cuda()
+    rd = StoryReader()
+    for raw in (False, True):
+        ts = []
+        for _ in range(a.reps):
+            t0 = time.perf_counter()
+            info = rd.parse_device(d.data_ptr(), d.numel(), raw=raw)
+            ts.append(time.perf_counter() - t0)
+        print("raw=%d n=%d bytes=%d nodes=%d median %.3f ms" % (raw, a.n, len(text), info.n_nodes,
+                                                                 1e3 * statistics.median(ts)))
+    rd.close()
+    return 0
+
+
+def energy_drift(argv):
+    """Energy conservation at scale: one N = 262144 Plummer sphere with
+    Salpeter masses (the bench's cluster), eps^2 = 1e-8, integrated from
+    t = 0 to --t with the device Hermite block-step integrator (eta = 0.02)
+    in the mixed and in the FP64 mode.  Energies of the initial and final
+    states from the engine's FP64 potential-only sweep (g6b200_energies),
+    the stand-in for the reference's hsys_stats -0 at a size where a CPU
+    run is out of reach.  Prints one JSON line."""
+    ap = argparse.ArgumentParser(prog="bench.py energy-drift")
+    ap.add_argument("--n", type=int, default=262144)
+    ap.add_argument("--t", type=float, default=1.0)
+    ap.add_argument("--eta", type=float, default=0.02)
+    ap.add_argument("--modes", default="mixed,fp64")
+    a = ap.parse_args(argv)
+    from starlab_b200 import G6Engine
+    from starlab_b200.ensemble import Ensemble
+    n = a.n
+    m, x, v = make_cluster(n, 11)
+
+    def energy(mm, xx, vv):
+        e = G6Engine(cluster_id=9, precision="fp64", npipes=n)
+        z = np.zeros((n, 3))
+        e.set_j_particles(0.0, mm, z, z, vv, xx)
+        e.set_ti(0.0)
+        ep, ek = e.energies(n, EPS2)
+        e.close()
+        return ep + ek
+
+    e0 = energy(m, x, v)
+    out = {"n": n, "eps2": EPS2, "eta": a.eta, "t_end": a.t, "E0": e0,
+           "energy_tool": "g6b200_energies, FP64 mode (potential-only sweep + device sums)"}
+    for mode in a.modes.split(","):
+        ens = Ensemble([m], [x], [v], EPS2, eta=a.eta, precision=mode)
+        ens.start()
+        st = ens.run(a.t)
+        f = ens.get(0)
+        ens.close()
+        e1 = energy(f["m"], f["x"], f["v"])
+        out[mode] = {"seconds": st["seconds"], "iterations": st["iterations"], "interactions": st["interactions"],
+                     "interactions_per_s": st["interactions"] / max(st["seconds"], 1e-9),
+                     "t_min": float(f["t"].min()), "t_max": float(f["t"].max()),
+                     "E1": e1, "dE_over_E": abs(e1 - e0) / abs(e0)}
+    if "mixed" in out and "fp64" in out:
+        out["mixed_over_fp64"] = out["mixed"]["dE_over_E"] / max(out["fp64"]["dE_over_E"], 1e-300)
+    print(json.dumps(out), flush=True)
+    return 0
+
+
+SUB_MODES = {"profile-case": profile_case, "profile-ensemble": profile_ensemble, "profile-story": profile_story,
+             "energy-drift": energy_drift}
+
+
 def main():
+    if len(sys.argv) > 1 and sys.argv[1] in SUB_MODES:
+        return SUB_MODES[sys.argv[1]](sys.argv[2:])
     args = parse()
     if args.impl == "reference":
         dist = Dist(use_cuda=False)
@@ -443,6 +636,11 @@ def main():
     dist.barrier()
     clocks = sampler.stop()
     launches = eng.stats()["launches"] - l0
+    # the last timed step's results, for the accuracy checks: the same sweep
+    # at the same block time, copied out
+    ti_last = dt * (args.warmup + args.steps)
+    eng.set_ti(ti_last)
+    gpu_last = eng.sweep(n, eps2=EPS2)
     total_ms = dist.max(sum(step_ms))
     interactions = n * (n - 1)
     value = weak_scaling_value(dist.world, interactions, args.steps, total_ms)
@@ -537,8 +735,11 @@ def main():
             line["grape4"] = grape4_section(7)
         if dist.world == 1 and not args.no_story:
             line["story"] = story_section(11, cpu=not args.no_cpu_baseline)
+        if dist.world == 1:
+            line["accuracy_vs_fp64_engine"] = accuracy_vs_fp64(m, x, v, acc, jerk, ti_last, gpu_last)
         if dist.world == 1 and not args.no_cpu_baseline:
-            line["cpu_baseline"] = cpu_baseline(n, seed, os.cpu_count() or 1, gpu=(acc, jerk, pot, nn))
+            line["cpu_baseline"] = cpu_baseline(n, seed, os.cpu_count() or 1, gpu=gpu_last,
+                                                state=(acc, jerk, ti_last))
         print(json.dumps(line), flush=True)
     for e in (eng, eng2, eng3):
         e.close()

@@ -120,10 +120,13 @@ def up_to_date(out, srcs):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", default=os.environ.get("STARLAB_REFERENCE"),
+                    help="root of the reference source tree (or STARLAB_REFERENCE); required")
     ap.add_argument("--jobs", type=int, default=os.cpu_count() or 4)
     ap.add_argument("--quiet", action="store_true")
     args = ap.parse_args()
+    if not args.ref:
+        ap.error("--ref (or STARLAB_REFERENCE) must name the reference source tree")
     src = os.path.join(args.ref, "src")
     if not os.path.isdir(src):
         print("reference tree not found at %s; skipping oracle/_ref build" % args.ref)
