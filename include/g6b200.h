@@ -337,6 +337,48 @@ int g6b200_split_finish(int cluster_id, long long nblocks_total, long long nj_to
                         double (*jerk)[3], double *pot, int *nn);
 int g6b200_set_position_range(int cluster_id, double xmax);
 
+/* Device-resident serving of many clusters' force calls (no counterpart in
+ * the reference, whose unit of work is one force_by_grape call,
+ * src/node/dyn/hdyn/evolve/hdyn_grape6.C:474-910).  One persistent
+ * cooperative kernel polls a ring of requests in pinned host memory,
+ * gathers every pending call into one batch (prediction of each call's
+ * j-set to its block time, one (call, i-tile, j-split) task list, results
+ * written back into the request's pinned buffer) and marks them done: no
+ * launch per call or per batch.  Every wait in the kernel is bounded by the
+ * global timer: it leaves after G6B200_RES_IDLE_MS (20) ms without calls and
+ * is launched again by the next submit; a grid barrier that does not
+ * complete within G6B200_RES_WAIT_MS (2000) ms ends it with an error and the
+ * calls it held fail with code 2.  Clusters are admitted against an HBM
+ * budget (open blocks until the footprint fits).  set_j waits until no call
+ * of the cluster is in flight and copies the touched j rows with the copy
+ * engine.  A call sees the j-particles set before it was submitted; its
+ * results are bit-identical alone and in any mix.  wait returns 0, 2 (the
+ * kernel left before the call completed), 3 (a j-tile copy wait timed out),
+ * 4 (positions outside the fixed-point range: the range is widened, submit
+ * again), < 0 (bad request).  hold(1) keeps calls from the kernel until
+ * hold(0) releases them together.  selftest_stall makes the kernel's CTA 0
+ * leave once without arriving at a barrier (the others' bounded waits run
+ * out: the failure path of the loop, without a GPU fault). */
+typedef struct g6b200_resident g6b200_resident;
+typedef struct {
+    long long batches, calls, launches, recoveries;
+    int max_batch;
+} g6b200_res_stats_t;
+g6b200_resident *g6b200_res_create(int device, long long hbm_budget_bytes, int precision, int max_batch);
+int g6b200_res_open_cluster(g6b200_resident *h, long long n_cap, double eps2);  /* cluster id or < 0 */
+int g6b200_res_close_cluster(g6b200_resident *h, int cluster);
+int g6b200_res_set_j(g6b200_resident *h, int cluster, int n, const int *address, const double *tj,
+                     const double *mass, const double (*j6)[3], const double (*a2)[3], const double (*v)[3],
+                     const double (*x)[3]);
+long long g6b200_res_submit(g6b200_resident *h, int cluster, double ti, int nj, int ni, const int *index,
+                            const double (*xi)[3], const double (*vi)[3]);  /* request id or < 0 */
+int g6b200_res_wait(g6b200_resident *h, long long request, double (*acc)[3], double (*jerk)[3], double *pot,
+                    int *nn, double *latency_s, long long *batch, int *batch_size);
+void g6b200_res_hold(g6b200_resident *h, int hold);
+void g6b200_res_selftest_stall(g6b200_resident *h);
+int g6b200_res_stats(g6b200_resident *h, g6b200_res_stats_t *out);
+void g6b200_res_destroy(g6b200_resident *h);
+
 /* Self-test of failure detection (no counterpart in the reference).  Every
  * j-tile copy the force kernel waits for is waited on with a time bound;
  * when a bound runs out the kernel sets a status bit and returns, and
