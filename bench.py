@@ -701,7 +701,15 @@ def main():
         peaks = measured_peaks()
         sm_max = float(peaks.get("sm_max_mhz", 1965.0))
         sms = props.multi_processor_count
-        peak_tflops = sms * 128 * 2 * sm_max * 1e6 / 1e12
+        nominal_tflops = sms * 128 * 2 * sm_max * 1e6 / 1e12
+        # the FP32 FMA rate measured on this GPU, after the timed region
+        import ctypes
+        from starlab_b200 import load_library
+        lib = load_library()
+        lib.g6b200_measure_fp32_peak.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
+        measured = ctypes.c_double(0)
+        peak_ok = lib.g6b200_measure_fp32_peak(dev, ctypes.byref(measured)) == 0 and measured.value > 0
+        peak_tflops = measured.value if peak_ok else nominal_tflops
         mean_force = statistics.mean(force_ms)
         achieved = FLOPS_PER_INTERACTION * interactions / (mean_force * 1e-3) / 1e12
         traffic = traffic_from_profile()
@@ -716,8 +724,12 @@ def main():
                          "frac": achieved / peak_tflops, "traffic": traffic,
                          "kernel": "force_kernel (mixed, + split reduction)",
                          "force_ms_mean": mean_force, "predict_ms_mean": statistics.mean(pred_ms),
-                         "peak_source": "derived: %d SMs x 128 FP32 lanes x 2 flops x %.0f MHz (max SM clock%s)"
-                                        % (sms, sm_max, ", MEASURED_PEAKS.json" if peaks else ", fallback")},
+                         "peak_source": ("measured in this run: packed FP32x2 FMA chains on every SM "
+                                         "(g6b200_measure_fp32_peak)" if peak_ok else
+                                         "derived (measurement failed)"),
+                         "peak_nominal": nominal_tflops,
+                         "peak_nominal_source": "%d SMs x 128 FP32 lanes x 2 flops x %.0f MHz (max SM clock%s)"
+                                                % (sms, sm_max, ", MEASURED_PEAKS.json" if peaks else ", fallback")},
             "e2e": {"value": e2e_value, "unit": "interactions/s", "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h), "steps": e2e_steps, "npipes": npipes,
                     "ms_per_step": e2e_s / e2e_steps * 1e3},

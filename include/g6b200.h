@@ -379,6 +379,12 @@ void g6b200_res_selftest_stall(g6b200_resident *h);
 int g6b200_res_stats(g6b200_resident *h, g6b200_res_stats_t *out);
 void g6b200_res_destroy(g6b200_resident *h);
 
+/* The FP32 FLOP rate this GPU sustains (no counterpart in the reference):
+ * a kernel of independent packed FP32x2 FMA chains on every SM, timed with
+ * CUDA events -- the measured denominator of the force kernel's roofline.
+ * Writes TFLOP/s; returns 0, or -1 on a CUDA error. */
+int g6b200_measure_fp32_peak(int device, double *tflops);
+
 /* Self-test of failure detection (no counterpart in the reference).  Every
  * j-tile copy the force kernel waits for is waited on with a time bound;
  * when a bound runs out the kernel sets a status bit and returns, and
