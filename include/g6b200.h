@@ -31,7 +31,11 @@
  *                      in two FP32 words so x_j - x_i is exact before its one
  *                      rounding to FP32; FP32 pair math with a Newton-refined
  *                      rsqrt; FP32 partial sums over short j-chunks folded
- *                      into FP64 accumulators.
+ *                      into FP64 accumulators; particles whose sums are ill
+ *                      conditioned (large, nearly cancelling terms: error
+ *                      indicators accumulated by the kernel) recomputed in
+ *                      FP64, so every particle meets acc, pot <= 1e-6 and
+ *                      jerk <= 1e-5 relative to FP64.
  */
 #ifndef G6B200_H
 #define G6B200_H
@@ -187,6 +191,7 @@ typedef struct {
     double last_predict_ms;
     double last_call_ms;
     long long launches;
+    long long refined;  /* mixed mode: particles recomputed in FP64 (ill-conditioned sums) */
 } g6b200_stats;
 int g6b200_get_stats(int cluster_id, g6b200_stats *out);
 

@@ -27,7 +27,7 @@ OBJDIR = os.path.join(PKG, "_build")
 LIB = os.path.join(LIBDIR, "libg6b200.so")
 LIB_H3 = os.path.join(LIBDIR, "libh3b200.so")
 H3_ONLY = {"grape4.o"}
-H3_OBJS = {"engine.o", "force.o", "predict.o", "nblist.o", "energy.o", "split.o", "grape4.o"}
+H3_OBJS = {"engine.o", "force.o", "predict.o", "nblist.o", "energy.o", "split.o", "refine.o", "grape4.o"}
 ORACLE_SRC = os.path.join(REPO, "oracle", "g6_oracle.c")
 ORACLE_LIB = os.path.join(REPO, "oracle", "_build", "libg6oracle.so")
 ORACLE_G4_SRC = os.path.join(REPO, "oracle", "g4_oracle.c")

@@ -305,6 +305,7 @@ int g6b200_get_stats(int cluster_id, g6b200_stats *out) {
     out->last_predict_ms = s.last_predict_ms;
     out->last_call_ms = s.last_call_ms;
     out->launches = s.launches;
+    out->refined = s.refined;
     return 0;
 }
 

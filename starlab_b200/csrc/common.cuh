@@ -57,7 +57,10 @@ struct __align__(16) Partial {
     double pot;
     double nn_r2;
     int nn_j;
-    int pad[3];
+    // Error indicators of the mixed mode's refinement (0 elsewhere):
+    // qa = sum over j of (m_j / r^2)^2, qj = sum over j of (m_j / r^3)^2.
+    float qa, qj;
+    int pad;
 };
 
 // i-particle input as uploaded by firsthalf (FP64 AoS, 64 B).

@@ -127,6 +127,11 @@ int Engine::open(int device, int nmax_hint) {
     G6_CHECK(cudaMalloc(&d_stage_index_, sizeof(int) * stage_cap_), "stage");
     G6_CHECK(cudaMalloc(&d_energy_, sizeof(double) * (2 * kEnergyBlocks + 2)), "energy");
     G6_CHECK(cudaMallocHost(&h_energy_, sizeof(double) * 2), "energy");
+    G6_CHECK(cudaMallocHost(&h_ref_count_, sizeof(int)), "refine");
+    *h_ref_count_ = 0;
+    G6_CHECK(cudaMalloc(&d_v2_, sizeof(double) * (kRefineBlocks + 1)), "refine");
+    G6_CHECK(cudaMalloc(&d_ref_small_, sizeof(int) * 8), "refine");
+    G6_CHECK(cudaMalloc(&d_ref_items_, sizeof(ForceParams)), "refine");
     open_ = true;
     if (ensure_capacity(std::max(nmax_hint, 1024) - 1)) return -1;
     return 0;
@@ -137,9 +142,10 @@ void Engine::close() {
     if (getenv("G6B200_TRACE")) {
         fprintf(stderr,
                 "g6b200[%d] trace: calls %lld interactions %lld launches %lld predictions %lld nb_calls %lld "
-                "pair_calls %lld range_retries %lld grows %lld wait_ms %.1f host_ms %.1f mode %d\n",
+                "pair_calls %lld refined %lld range_retries %lld grows %lld wait_ms %.1f host_ms %.1f mode %d\n",
                 cluster_id_, stats_.calls, stats_.interactions, stats_.launches, stats_.predictions, stats_.nb_calls,
-                stats_.pair_calls, stats_.range_retries, stats_.grows, stats_.wait_ms, stats_.host_ms, mode_);
+                stats_.pair_calls, stats_.refined, stats_.range_retries, stats_.grows, stats_.wait_ms, stats_.host_ms,
+                mode_);
     }
     cudaSetDevice(device_);
     cudaStreamSynchronize(stream_);
@@ -152,6 +158,13 @@ void Engine::close() {
     hfree(h_stage_vals_); hfree(h_stage_addr_); hfree(h_stage_index_);
     hfree(h_irec_); hfree(h_out_); hfree(h_nb_off_); hfree(h_nb_count_); hfree(h_bulk_);
     hfree(h_ieps2_); dfree(d_ieps2_); hfree(h_energy_); dfree(d_energy_);
+    hfree(h_ref_count_); dfree(d_v2_); dfree(d_ref_small_); dfree(d_ref_items_); dfree(d_q_);
+    dfree(d_ref_list_); dfree(d_ref_tcnt_); dfree(d_ref_nn_); dfree(d_ref_irec_); dfree(d_ref_out_);
+    dfree(d_ref_part_); dfree(d_jrec64_);
+    h_ref_count_ = nullptr; d_v2_ = nullptr; d_ref_small_ = nullptr; d_ref_items_ = nullptr; d_q_ = nullptr;
+    d_ref_list_ = nullptr; d_ref_tcnt_ = nullptr; d_ref_nn_ = nullptr; d_ref_irec_ = nullptr; d_ref_out_ = nullptr;
+    d_ref_part_ = nullptr; d_jrec64_ = nullptr; ref_cap_ = 0; jrec64_cap_ = 0;
+    pred64_valid_ = v2_valid_ = false;
     cudaEvent_t evs[] = {ev_stage_, ev_begin_, ev_pred0_, ev_pred1_, ev_force0_, ev_force1_, ev_done_};
     for (cudaEvent_t e : evs) if (e) cudaEventDestroy(e);
     if (ev_ext_) cudaEventDestroy(ev_ext_);
@@ -498,6 +511,39 @@ int Engine::ensure_call_buffers(int ni, bool nb, size_t part_bytes) {
     return 0;
 }
 
+// Buffers of the mixed mode's FP64 refinement for calls of up to ni i (and
+// FP64 j-records for the j-memory's capacity).
+int Engine::ensure_refine_buffers(int ni) {
+    if (ni > ref_cap_) {
+        const int n = std::max(ni, npipes_);
+        auto dfree = [](void *p) { if (p) cudaFree(p); };
+        dfree(d_q_); dfree(d_ref_list_); dfree(d_ref_tcnt_); dfree(d_ref_nn_); dfree(d_ref_irec_);
+        dfree(d_ref_out_); dfree(d_ref_part_);
+        d_q_ = nullptr; d_ref_list_ = d_ref_tcnt_ = d_ref_nn_ = nullptr; d_ref_irec_ = nullptr;
+        d_ref_out_ = nullptr; d_ref_part_ = nullptr;
+        ref_cap_ = 0;
+        G6_CHECK(cudaMalloc(&d_q_, sizeof(float) * 2 * (size_t)n), "refine");
+        G6_CHECK(cudaMalloc(&d_ref_list_, sizeof(int) * (size_t)n), "refine");
+        G6_CHECK(cudaMalloc(&d_ref_tcnt_, sizeof(int) * (size_t)n), "refine");
+        G6_CHECK(cudaMemsetAsync(d_ref_tcnt_, 0, sizeof(int) * (size_t)n, stream_), "refine");
+        G6_CHECK(cudaMalloc(&d_ref_nn_, sizeof(int) * (size_t)n), "refine");
+        G6_CHECK(cudaMalloc(&d_ref_irec_, sizeof(IRec) * (size_t)n), "refine");
+        G6_CHECK(cudaMalloc(&d_ref_out_, sizeof(double) * 7 * (size_t)n), "refine");
+        G6_CHECK(cudaMalloc(&d_ref_part_, sizeof(Partial) * refine_partial_records(n)), "refine");
+        ref_cap_ = n;
+        stats_.grows++;
+    }
+    if (jrec64_cap_ < cap_) {
+        if (d_jrec64_) cudaFree(d_jrec64_);
+        d_jrec64_ = nullptr;
+        jrec64_cap_ = 0;
+        G6_CHECK(cudaMalloc(&d_jrec64_, sizeof(JRecF64) * (size_t)cap_), "refine");
+        jrec64_cap_ = cap_;
+        pred64_valid_ = false;
+    }
+    return 0;
+}
+
 int Engine::firsthalf(int nj, int ni, const int *index, const double (*xi)[3], const double (*vi)[3],
                       double eps2, const double *h2) {
     return firsthalf_impl(nj, ni, index, xi, vi, eps2, nullptr, h2);
@@ -604,6 +650,7 @@ int Engine::firsthalf_impl(int nj, int ni, const int *index, const double (*xi)[
 
 int Engine::launch_call() {
     const int ni = call_ni_, nj = call_nj_;
+    call_refine_ = false;
     const int km = kmode();
     const int T = tile_size(km);
     const int nj_pad = round_up(nj, T);
@@ -631,6 +678,7 @@ int Engine::launch_call() {
     pred_timed_ = false;
     const bool need_pred = !pred_valid_ || pred_ti_ != ti_ || pred_nj_ != nj || pred_mode_ != km || pred_E_ != E_ ||
                            (small && n_staged_ > 0);
+    if (need_pred) pred64_valid_ = v2_valid_ = false;  // the refinement's FP64 records and |v| scale follow
     if (small) {
         // Updates, prediction and i-records in one launch whose parameter is
         // the call's host data (no host->device copy).
@@ -709,6 +757,11 @@ int Engine::launch_call() {
         // FP64 layouts; the scalar mixed layout runs its full kernel.
         const bool pot_k = call_pot_ && km != kKernMixedDS;
         if (pot_k) cfg.r = 1;
+        // Mixed mode (paired layout): ill-conditioned particles are
+        // recomputed in FP64 (refine.cu); not for potential-only, j-split
+        // or GRAPE-4 calls.
+        call_refine_ = km == kKernMixedP && !pot_k && !call_split_ && !call_g4_;
+        if (call_refine_ && ensure_refine_buffers(ni)) return -1;
         if (call_split_) cfg.jper = call_split_;
         if (ensure_call_buffers(ni, call_nb_, call_split_ ? partial_bytes_fixed(call_split_, nj_pad, ni)
                                                           : partial_bytes(cfg, ni)))
@@ -735,12 +788,58 @@ int Engine::launch_call() {
         p.tile_counter = call_split_ ? nullptr : d_tile_cnt_;
         p.ieps2 = call_g4_ ? d_ieps2_ : nullptr;
         p.keep_partials = call_split_ ? 1 : 0;
+        p.out_q = call_refine_ ? d_q_ : nullptr;
         if (call_nb_) G6_CHECK(cudaMemsetAsync(d_nb_count_, 0, sizeof(int) * ni, stream_), "memset");
         if (timed_) G6_CHECK(cudaEventRecord(ev_force0_, stream_), "event");
         G6_CHECK(launch_force(stream_, km, cfg, p, n_nonident_ == 0 && !call_g4_, call_nb_, call_g4_, pot_k),
                  "force launch");
         if (timed_) G6_CHECK(cudaEventRecord(ev_force1_, stream_), "event");
         stats_.launches += 1;
+        if (call_refine_) {
+            if (!v2_valid_) {
+                launch_refine_v2(stream_, d_jraw_, cap_, nj, d_v2_);
+                G6_CHECK(cudaGetLastError(), "refine launch");
+                stats_.launches += 2;
+                v2_valid_ = true;
+            }
+            if (!pred64_valid_) {
+                launch_predict(stream_, kKernF64, d_jraw_, d_jindex_, cap_, nj, nj_pad, ti_, fs, d_jrec64_, status);
+                G6_CHECK(cudaGetLastError(), "refine predict launch");
+                stats_.launches++;
+                pred64_valid_ = true;
+            }
+            RefineArgs ra{};
+            ra.ni = ni;
+            ra.nj = nj;
+            ra.nj_pad = round_up(nj, tile_size(kKernF64));
+            ra.ident = n_nonident_ == 0;
+            ra.eps2 = call_eps2_;
+            ra.v2 = d_v2_;
+            ra.q = d_q_;
+            ra.irec = d_irec_;
+            ra.jrec64 = d_jrec64_;
+            ra.acc = p.out_acc;
+            ra.jerk = p.out_jerk;
+            ra.pot = p.out_pot;
+            ra.nn = p.out_nn;
+            ra.count = d_ref_small_;
+            ra.counter = d_ref_small_ + 1;
+            ra.pre = d_ref_small_ + 2;
+            ra.list = d_ref_list_;
+            ra.irec_ref = d_ref_irec_;
+            ra.racc = d_ref_out_;
+            ra.rjerk = d_ref_out_ + 3 * (size_t)ref_cap_;
+            ra.rpot = d_ref_out_ + 6 * (size_t)ref_cap_;
+            ra.rnn = d_ref_nn_;
+            ra.part = d_ref_part_;
+            ra.tcnt = d_ref_tcnt_;
+            ra.items = d_ref_items_;
+            ra.status = status;
+            G6_CHECK(launch_refine(stream_, ra, num_sms_), "refine launch");
+            stats_.launches += 5;
+            G6_CHECK(cudaMemcpyAsync(h_ref_count_, d_ref_small_, sizeof(int), cudaMemcpyDeviceToHost, stream_),
+                     "refine count");
+        }
         if (call_split_) {
             split_nsplit_ = std::max(1, (nj_pad + call_split_ - 1) / call_split_);
             launch_split_agree(stream_, ni, split_nsplit_, d_part_, split_agree_);
@@ -833,6 +932,7 @@ int Engine::wait_call() {
         }
         break;
     }
+    if (call_refine_) stats_.refined += *h_ref_count_;
     float ms = 0;
     if (!timed_) {
         stats_.last_force_ms = stats_.last_predict_ms = stats_.last_call_ms = 0;

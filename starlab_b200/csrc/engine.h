@@ -23,6 +23,7 @@ struct EngineStats {
     // (hdyn_grape6.C:3415-3587 sends both components with their top-level
     // node's index)
     long long pair_calls = 0;
+    long long refined = 0;  // mixed mode: particles recomputed in FP64 (ill-conditioned sums)
     double wait_ms = 0, host_ms = 0;
 };
 
@@ -238,6 +239,24 @@ class Engine {
     bool call_energy_ = false;  // + the energy reduction (sweeps)
     bool call_copy_ = true;
     double *d_energy_ = nullptr;  // [2 * kEnergyBlocks + 2] block partials, then epot, ekin
+    // mixed-mode FP64 refinement (refine.cu)
+    int ensure_refine_buffers(int ni);
+    int ref_cap_ = 0;
+    float *d_q_ = nullptr;            // [ref_cap_][2] error indicators
+    int *d_ref_list_ = nullptr, *d_ref_tcnt_ = nullptr, *d_ref_nn_ = nullptr;
+    IRec *d_ref_irec_ = nullptr;
+    double *d_ref_out_ = nullptr;     // acc [3 cap], jerk [3 cap], pot [cap]
+    Partial *d_ref_part_ = nullptr;
+    ForceParams *d_ref_items_ = nullptr;
+    int *d_ref_small_ = nullptr;      // count, counter, pre[4]
+    double *d_v2_ = nullptr;          // [kRefineBlocks + 1]
+    void *d_jrec64_ = nullptr;        // FP64 records of the refinement [cap_]
+    int jrec64_cap_ = 0;
+    bool pred64_valid_ = false, v2_valid_ = false;
+    double pred64_ti_ = 0;
+    int pred64_nj_ = -1, v2_nj_ = -1;
+    int *h_ref_count_ = nullptr;      // pinned
+    bool call_refine_ = false;
     double *h_energy_ = nullptr;  // pinned: epot, ekin
     int call_i0_ = 0;
     ForceConfig last_cfg_{};

@@ -148,7 +148,9 @@ using KernelFn = void (*)(const ForceParams);
 
 template <int K, int IL, int R>
 static KernelFn pick3(bool nb, bool ident) {
-    constexpr int V = kVarUnroll4;
+    // the single-call paired mixed kernels also accumulate the refinement's
+    // error indicators
+    constexpr int V = kVarUnroll4 | (K == kKernMixedP ? kVarStats : 0);
     if (nb) return ident ? force_kernel<K, IL, R, true, true, V> : force_kernel<K, IL, R, true, false, V>;
     return ident ? force_kernel<K, IL, R, false, true, V> : force_kernel<K, IL, R, false, false, V>;
 }

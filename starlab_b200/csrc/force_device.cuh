@@ -249,6 +249,7 @@ struct StateMixedP {
     float2 nxh, nyh, nzh, nxl, nyl, nzl, nvx, nvy, nvz;
     float h2;
     float2 ax, ay, az, jx, jy, jz, pm;  // FP32 sums since the last fold; pm = sum m/(4r)
+    float2 qa, qj;                      // error indicators (kVarStats): sum (m/r^2)^2, sum (m/r^3)^2
     double Ax, Ay, Az, Jx, Jy, Jz, Pt;
     float nr2;
     int nj, idx, i;
@@ -274,12 +275,13 @@ __device__ __forceinline__ void load_i(StateMixedP &s, const IRec &q, const Forc
     s.h2 = (float)q.h2;
     s.idx = q.index;
     s.ax = s.ay = s.az = s.jx = s.jy = s.jz = s.pm = make_float2(0.f, 0.f);
+    s.qa = s.qj = make_float2(0.f, 0.f);
     s.Ax = s.Ay = s.Az = s.Jx = s.Jy = s.Jz = s.Pt = 0.0;
     s.nr2 = FLT_MAX;
     s.nj = -1;
 }
 
-template <bool CHK, bool NB, bool IDENT, bool PO = false>
+template <bool CHK, bool NB, bool IDENT, bool PO = false, bool STATS = false>
 __device__ __forceinline__ void interact_pair(StateMixedP &s, const JPairMixed &J, int jg0, float2 eps2,
                                               const ForceParams &p) {
     if constexpr (PO) {
@@ -346,6 +348,13 @@ __device__ __forceinline__ void interact_pair(StateMixedP &s, const JPairMixed &
     const float2 mr = __fmul2_rn(m, y);
     const float2 mr3 = __fmul2_rn(mr, r2inv);
     const float2 a3 = __fmul2_rn(__fmul2_rn(rv, dup(-0.75f)), r2inv);
+    if (STATS) {
+        // the refinement's error indicators: mr3 = m / r^3 exactly (see
+        // above), so u r2 = (m / r^2)^2 and u = (m / r^3)^2 (self: m = 0)
+        const float2 u = __fmul2_rn(mr3, mr3);
+        s.qa = __ffma2_rn(u, r2, s.qa);
+        s.qj = __fadd2_rn(s.qj, u);
+    }
     s.pm = __fadd2_rn(s.pm, mr);
     s.ax = __ffma2_rn(mr3, dx, s.ax);
     s.ay = __ffma2_rn(mr3, dy, s.ay);
@@ -412,6 +421,9 @@ constexpr int kVarUnroll4 = 2;
 constexpr int kVarG4 = 4;
 // 8 = potential only (paired mixed and FP64 layouts): the energy sweeps.
 constexpr int kVarPot = 8;
+// 16 = paired mixed layout: also accumulate the refinement's error
+// indicators (two FP32x2 sums, three instructions per pair of j).
+constexpr int kVarStats = 16;
 
 // Consume one shared-memory tile: this thread's j are kbase + m*JL.
 template <int K, int R, int JL, bool CHK, bool NB, bool IDENT, int V>
@@ -420,6 +432,7 @@ __device__ __forceinline__ void consume_tile(typename StateOf<K>::type (&st)[R],
                                              int per, int tb, const ForceParams &p) {
     if constexpr (K == kKernMixedP) {
         constexpr bool PO = (V & kVarPot) != 0;
+        constexpr bool ST = (V & kVarStats) != 0;
         const float2 eps2 = dup((float)p.eps2);
         constexpr int kFlushPairs = kFlush / 2;
         if constexpr (kFlushPairs <= 2) {
@@ -433,7 +446,7 @@ __device__ __forceinline__ void consume_tile(typename StateOf<K>::type (&st)[R],
                         const JPairMixed J = S[k];
 #pragma unroll
                         for (int r = 0; r < R; ++r)
-                            interact_pair<CHK, NB, IDENT, PO>(st[r], J, tb + 2 * k, eps2, p);
+                            interact_pair<CHK, NB, IDENT, PO, ST>(st[r], J, tb + 2 * k, eps2, p);
                     }
                 }
 #pragma unroll
@@ -448,7 +461,7 @@ __device__ __forceinline__ void consume_tile(typename StateOf<K>::type (&st)[R],
                 const int k = kbase + m * JL;
                 const JPairMixed J = S[k];
 #pragma unroll
-                for (int r = 0; r < R; ++r) interact_pair<CHK, NB, IDENT, PO>(st[r], J, tb + 2 * k, eps2, p);
+                for (int r = 0; r < R; ++r) interact_pair<CHK, NB, IDENT, PO, ST>(st[r], J, tb + 2 * k, eps2, p);
             }
 #pragma unroll
             for (int r = 0; r < R; ++r) fold_any<PO>(st[r]);
@@ -512,6 +525,7 @@ __device__ __forceinline__ void to_partial(const StateMixedBase &s, Partial &q) 
     q.pot = s.Pt;
     q.nn_r2 = (double)s.nr2;
     q.nn_j = s.nj;
+    q.qa = q.qj = 0.f;
 }
 __device__ __forceinline__ void to_partial(const StateMixedP &s, Partial &q) {
     q.acc[0] = s.Ax; q.acc[1] = s.Ay; q.acc[2] = s.Az;
@@ -519,6 +533,8 @@ __device__ __forceinline__ void to_partial(const StateMixedP &s, Partial &q) {
     q.pot = s.Pt;
     q.nn_r2 = (double)s.nr2;
     q.nn_j = s.nj;
+    q.qa = s.qa.x + s.qa.y;
+    q.qj = s.qj.x + s.qj.y;
 }
 __device__ __forceinline__ void to_partial(const StateF64 &s, Partial &q) {
     q.acc[0] = s.Ax; q.acc[1] = s.Ay; q.acc[2] = s.Az;
@@ -526,6 +542,7 @@ __device__ __forceinline__ void to_partial(const StateF64 &s, Partial &q) {
     q.pot = s.Pt;
     q.nn_r2 = s.nr2;
     q.nn_j = s.nj;
+    q.qa = q.qj = 0.f;
 }
 
 __device__ __forceinline__ void add_partial(Partial &a, const Partial &b) {
@@ -536,6 +553,8 @@ __device__ __forceinline__ void add_partial(Partial &a, const Partial &b) {
     }
     a.pot += b.pot;
     take_min(a.nn_r2, a.nn_j, b.nn_r2, b.nn_j);
+    a.qa += b.qa;
+    a.qj += b.qj;
 }
 
 // Sum over the lanes of a warp that share an i (lane bits >= log2(IL)).
@@ -552,6 +571,8 @@ __device__ __forceinline__ void warp_reduce(Partial &q) {
         o.pot = __shfl_xor_sync(0xffffffffu, q.pot, off);
         o.nn_r2 = __shfl_xor_sync(0xffffffffu, q.nn_r2, off);
         o.nn_j = __shfl_xor_sync(0xffffffffu, q.nn_j, off);
+        o.qa = __shfl_xor_sync(0xffffffffu, q.qa, off);
+        o.qj = __shfl_xor_sync(0xffffffffu, q.qj, off);
         add_partial(q, o);
     }
 }
@@ -567,6 +588,8 @@ __device__ __forceinline__ Partial load_partial_cg(const Partial *src) {
     a.pot = __ldcg(&src->pot);
     a.nn_r2 = __ldcg(&src->nn_r2);
     a.nn_j = __ldcg(&src->nn_j);
+    a.qa = __ldcg(&src->qa);
+    a.qj = __ldcg(&src->qj);
     return a;
 }
 
@@ -578,6 +601,10 @@ __device__ __forceinline__ void write_final(const ForceParams &p, int i, const P
     }
     p.out_pot[i] = q.pot;
     p.out_nn[i] = (q.nn_j < 0 || q.nn_j >= p.nj) ? 0 : q.nn_j;
+    if (p.out_q) {
+        p.out_q[2 * (size_t)i] = q.qa;
+        p.out_q[2 * (size_t)i + 1] = q.qj;
+    }
 }
 
 // Resident CTAs per SM the register budget is sized for (3 for the paired

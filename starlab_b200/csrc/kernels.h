@@ -69,6 +69,9 @@ struct ForceParams {
     // 1: every split's partial sums stay in part[split][i] (also for one
     // split) and are not folded: the multi-GPU j-split combines them.
     int keep_partials;
+    // Mixed-mode error indicators (qa, qj of Partial) per i, [ni][2], when
+    // the kernel accumulates them (single-call paired mixed kernels).
+    float *out_q;
 };
 
 // A batch of calls for the persistent multi-item kernel (device pointers).
@@ -238,6 +241,35 @@ void launch_split_fix(cudaStream_t s, int ni, int nsplit, int g, long long j_off
 void launch_split_finish(cudaStream_t s, int ni, int g, long long nj_total, const long long *agree,
                          const long long *sums, const long long *negj, double *acc, double *jerk, double *pot,
                          int *nn);
+
+// Mixed-mode FP64 refinement (refine.cu): particles whose error indicators
+// (ForceParams::out_q) exceed the bounds below are recomputed in FP64.
+constexpr double kRefineA = 1.0;  // sqrt(sum (m/r^2)^2) / |acc|
+constexpr double kRefineJ = 3.0;  // sqrt(sum (m/r^3)^2) v_rms / |jerk|
+constexpr int kRefineBlocks = 256;
+struct RefineArgs {
+    int ni, nj, nj_pad, ident;
+    double eps2;
+    const double *v2;         // [kRefineBlocks + 1]: mean |v|^2 of the j-set in the last entry
+    const float *q;           // [ni][2] error indicators
+    const IRec *irec;         // [ni] the call's i-records
+    const void *jrec64;       // JRecF64 [nj_pad] at the call's block time
+    double *acc, *jerk, *pot; // the call's outputs, refined in place
+    int *nn;
+    int *count, *list;        // flagged count, [ni] flagged i
+    IRec *irec_ref;           // [ni]
+    double *racc, *rjerk, *rpot;  // [ni] FP64 pass outputs
+    int *rnn;
+    Partial *part;            // refine_partial_records(ni)
+    int *tcnt;                // [ni] i-tile counters, zero between calls
+    ForceParams *items;       // [1]
+    int *pre;                 // [4]
+    int *counter;
+    unsigned *status;
+};
+void launch_refine_v2(cudaStream_t s, const double *jraw, int cap, int nj, double *work);
+cudaError_t launch_refine(cudaStream_t s, const RefineArgs &r, int num_sms);
+size_t refine_partial_records(int ni);
 
 // Neighbour lists: per-i sort + compaction into ascending address order.
 // offsets[ni+1] (exclusive scan of min(count, cap)), out[total].

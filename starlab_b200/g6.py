@@ -39,7 +39,7 @@ class Stats(ctypes.Structure):
                 ("j_updates", ctypes.c_longlong), ("h2d_bytes", ctypes.c_longlong),
                 ("d2h_bytes", ctypes.c_longlong), ("last_force_ms", ctypes.c_double),
                 ("last_predict_ms", ctypes.c_double), ("last_call_ms", ctypes.c_double),
-                ("launches", ctypes.c_longlong)]
+                ("launches", ctypes.c_longlong), ("refined", ctypes.c_longlong)]
 
 
 _lib = None

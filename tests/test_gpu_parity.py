@@ -266,3 +266,59 @@ def test_deterministic_repeat(c2):
     for a, b in zip(r1, r2):
         assert np.array_equal(a, b)
     eng.close()
+
+
+def _all_i_errors(n, seed, eps2, ti, masses=None):
+    """Every particle of an n-body snapshot at a predicted block time, mixed
+    mode against the engine's FP64 mode (itself within 1e-12 of the oracle:
+    checked on a sample here too).  acc and jerk for the predictor from one
+    FP64 sweep at t = 0."""
+    from starlab_b200 import ics
+    m, x, v = ics.plummer(n, seed, masses=masses)
+    z = np.zeros((n, 3))
+    e64 = new_engine("fp64", npipes=n)
+    e64.set_j_particles(0.0, m, z, z, v, x)
+    e64.set_ti(0.0)
+    acc, jerk, _, _ = e64.sweep(n, eps2=eps2)
+    e64.set_j_particles(0.0, m, jerk / 6.0, 0.5 * acc, v, x)
+    e64.set_ti(ti)
+    ref = e64.sweep(n, eps2=eps2)
+    emx = new_engine("mixed", npipes=n)
+    emx.set_j_particles(0.0, m, jerk / 6.0, 0.5 * acc, v, x)
+    emx.set_ti(ti)
+    got = emx.sweep(n, eps2=eps2)
+    refined = emx.stats()["refined"]
+    e64.close()
+    emx.close()
+    return (m, x, v, acc, jerk), got, ref, refined
+
+
+@pytest.mark.parametrize("case", ["c2", "c3"])
+def test_mixed_every_particle_within_tolerance(case, oracle):
+    """The precision contract on EVERY particle, not a sample: acc and pot
+    within 1e-6 and jerk within 1e-5 of FP64 for all 65536 particles of the
+    single-call sweep configuration and all 262144 of the N = 262144
+    Plummer/Salpeter configuration, at a predicted block time.  The mixed
+    mode's refinement recomputes the ill-conditioned particles in FP64; the
+    number it recomputed is reported."""
+    from starlab_b200 import ics
+    if case == "c2":
+        state, got, ref, refined = _all_i_errors(65536, 7, EPS2, TI)
+    else:
+        n = 262144
+        state, got, ref, refined = _all_i_errors(n, 11, 1e-8, 1.0 / 1024, masses=ics.salpeter_masses(n, 12))
+    ea, ej, ep = rel_err_vec(got[0], ref[0]), rel_err_vec(got[1], ref[1]), rel_err(got[2], ref[2])
+    print("%s: acc median %.2e max %.2e | jerk median %.2e max %.2e | pot median %.2e max %.2e | refined %d"
+          % (case, np.median(ea), ea.max(), np.median(ej), ej.max(), np.median(ep), ep.max(), refined))
+    assert ea.max() <= 1e-6, (float(ea.max()), int(ea.argmax()))
+    assert ej.max() <= 1e-5, (float(ej.max()), int(ej.argmax()))
+    assert ep.max() <= 1e-6, float(ep.max())
+    assert refined < 0.05 * len(ea)
+    # the FP64 reference itself against the oracle on a sample
+    m, x, v, acc, jerk = state
+    eps2 = EPS2 if case == "c2" else 1e-8
+    ti = TI if case == "c2" else 1.0 / 1024
+    xp, vp = oracle.predict(ti, 0.0, x, v, 0.5 * acc, jerk / 6.0)
+    samp = np.linspace(0, len(m) - 1, 64).astype(np.int32)
+    ra, rj, rp, _, _ = oracle.force(xp, vp, m, samp, xp[samp], vp[samp], eps2)
+    assert rel_err_vec(ref[0][samp], ra).max() < 1e-12 and rel_err(ref[2][samp], rp).max() < 1e-12
