@@ -208,28 +208,36 @@ def served_section(seed, rates=(2000.0, 20000.0), n_calls=3000):
     configured 2000 calls/s and at a rate well above what one call at a time
     can serve (the queue then builds and batches fill)."""
     from starlab_b200 import G6Engine
-    from starlab_b200.server import Server
+    from starlab_b200.server import ResidentServer, Server
     from starlab_b200.stream import make_clusters, make_stream, run_served, run_sequential
     clusters = make_clusters(48, seed)
-    out = {"clusters": len(clusters), "calls": n_calls}
+    out = {"clusters": len(clusters), "calls": n_calls,
+           "servers": {"served": "g6b200_srv_*: host dispatch lanes, one batched launch per batch",
+                       "resident": "g6b200_res_*: one persistent kernel polling a request ring, no launches"}}
+
+    def summary(lat, wall, inter, st=None):
+        d = {"p50_ms": float(np.percentile(lat, 50) * 1e3), "p99_ms": float(np.percentile(lat, 99) * 1e3),
+             "interactions_per_s": inter / wall, "wall_s": wall}
+        if st is not None:
+            d.update(batches=st["batches"], mean_batch=st["requests"] / max(1, st["batches"]),
+                     max_batch=st["max_batch"])
+        return d
+
     for rate in rates:
         calls = make_stream(clusters, rate, n_calls, seed)
-        srv = Server(precision="mixed")
-        lat, wall, inter = run_served(srv, clusters, calls)
-        st = srv.stats()
-        srv.close()
+        row = {"rate_per_s": rate}
+        for key, make in (("served", lambda: Server(precision="mixed")),
+                          ("resident", lambda: ResidentServer(precision="mixed"))):
+            srv = make()
+            lat, wall, inter = run_served(srv, clusters, calls)
+            row[key] = summary(lat, wall, inter, srv.stats())
+            srv.close()
         lat2, wall2, inter2 = run_sequential(
             lambda k, n: G6Engine(cluster_id=3000 + k, precision="mixed", npipes=n), clusters, calls)
-        out["rate_%d" % int(rate)] = {
-            "rate_per_s": rate,
-            "served": {"p50_ms": float(np.percentile(lat, 50) * 1e3), "p99_ms": float(np.percentile(lat, 99) * 1e3),
-                       "interactions_per_s": inter / wall, "batches": st["batches"],
-                       "mean_batch": st["requests"] / max(1, st["batches"]), "max_batch": st["max_batch"],
-                       "wall_s": wall},
-            "one_call_at_a_time": {"p50_ms": float(np.percentile(lat2, 50) * 1e3),
-                                   "p99_ms": float(np.percentile(lat2, 99) * 1e3),
-                                   "interactions_per_s": inter2 / wall2, "wall_s": wall2},
-            "served_over_plain": (inter / wall) / (inter2 / wall2)}
+        row["one_call_at_a_time"] = summary(lat2, wall2, inter2)
+        for key in ("served", "resident"):
+            row[key + "_over_plain"] = row[key]["interactions_per_s"] / row["one_call_at_a_time"]["interactions_per_s"]
+        out["rate_%d" % int(rate)] = row
     return out
 
 
