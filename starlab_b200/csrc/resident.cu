@@ -932,7 +932,11 @@ int Resident::wait(long long id, double (*acc)[3], double (*jerk)[3], double *po
                 return -3;
             }
         }
-        if (spin > 2048) std::this_thread::yield();
+        // spin briefly, then yield, then nap (many client threads may wait at once)
+        if (spin > 20000)
+            std::this_thread::sleep_for(std::chrono::microseconds(20));
+        else if (spin > 2048)
+            std::this_thread::yield();
     }
     const double t_done = now_s();
     const int ni = s.ni;
