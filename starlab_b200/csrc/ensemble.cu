@@ -741,20 +741,41 @@ int Ensemble::run_batched(double t_end, EnsembleStats *st, int tune) {
     ECHK(cudaStreamEndCapture(stream_, &g), "capture");
     ECHK(cudaGraphInstantiate(&graph_, g, 0), "instantiate");
     cudaGraphDestroy(g);
-    ECHK(cudaMallocHost(&sc.h_active, sizeof(int)), "pinned");
+    // Two graph launches in flight: while the GPU runs one, the host waits
+    // for the other's active-cluster count, so the GPU never idles on the
+    // host's check.  Once every cluster has finished, the launch already in
+    // flight runs iterations with no active cluster (no work, no change).
+    ECHK(cudaMallocHost(&sc.h_active, 2 * sizeof(int)), "pinned");
     int *h_active = sc.h_active;
-    for (;;) {
+    cudaEvent_t done[2];
+    for (cudaEvent_t &e : done) ECHK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "event");
+    struct Events {
+        cudaEvent_t *e;
+        ~Events() {
+            cudaEventDestroy(e[0]);
+            cudaEventDestroy(e[1]);
+        }
+    } ev_guard{done};
+    auto launch = [&](int slot) -> int {
         ECHK(cudaGraphLaunch(graph_, stream_), "graph launch");
         iters += K;
-        cudaMemcpyAsync(h_active, d_.active, sizeof(int), cudaMemcpyDeviceToHost, stream_);
-        ECHK(cudaStreamSynchronize(stream_), "run");
-        if (*h_active == 0) break;
+        ECHK(cudaMemcpyAsync(h_active + slot, d_.active, sizeof(int), cudaMemcpyDeviceToHost, stream_), "copy");
+        ECHK(cudaEventRecord(done[slot], stream_), "event");
+        return 0;
+    };
+    if (launch(0)) return -1;
+    for (int slot = 0;; slot ^= 1) {
+        if (launch(slot ^ 1)) return -1;
+        ECHK(cudaEventSynchronize(done[slot]), "run");
+        if (h_active[slot] == 0) break;
         if (iters > max_iters_ ||
             std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count() > max_seconds_) {
+            cudaStreamSynchronize(stream_);
             err = "ensemble: iteration or time limit reached";
             return -1;
         }
     }
+    ECHK(cudaStreamSynchronize(stream_), "run");
     auto t1 = std::chrono::steady_clock::now();
     unsigned long long i1 = 0;
     unsigned status = 0;
