@@ -7,7 +7,8 @@ v_i^2 on the host.  g6b200_calc_pot runs a potential-only kernel and
 g6b200_energies forms both sums on the device.  Checked against the FP64
 oracle (FP64 mode <= 1e-12; mixed mode <= 1e-6), and the mixed mode's
 potential-only kernel against the full kernel's pot (the same rounding
-sequence: bit-identical).
+sequence: bit-identical except where the full call's refinement recomputed
+a particle in FP64).
 """
 import numpy as np
 import pytest
@@ -42,7 +43,11 @@ def test_potential_only_matches_oracle_and_full_kernel(mode, oracle):
         assert err.max() <= TOL[mode], (ni, float(err.max()))
         full = eng.force(n, idx, xp[idx], vp[idx], EPS2)[2]
         if mode == "mixed":
-            assert np.array_equal(pot.view(np.uint64), full.view(np.uint64)), ni
+            # the same rounding sequence; the full call's refinement replaces
+            # its ill-conditioned particles (about 1%) by FP64 values
+            same = pot.view(np.uint64) == full.view(np.uint64)
+            assert same.mean() >= 0.95, (ni, float(same.mean()))
+            assert (np.abs(pot - full) / np.abs(full)).max() <= 1e-6
         else:
             assert np.abs(pot - full).max() <= 1e-13 * np.abs(full).max()
     st = eng.stats()
