@@ -57,8 +57,8 @@ struct __align__(16) Partial {
     double pot;
     double nn_r2;
     int nn_j;
-    // Error indicators of the mixed mode's refinement (0 elsewhere):
-    // qa = sum over j of (m_j / r^2)^2, qj = sum over j of (m_j / r^3)^2.
+    // Error indicators of the mixed mode's refinement (0 elsewhere): the
+    // largest single terms, qa = max over j of m_j / r^2, qj = max of m_j / r^3.
     float qa, qj;
     int pad;
 };

@@ -249,7 +249,7 @@ struct StateMixedP {
     float2 nxh, nyh, nzh, nxl, nyl, nzl, nvx, nvy, nvz;
     float h2;
     float2 ax, ay, az, jx, jy, jz, pm;  // FP32 sums since the last fold; pm = sum m/(4r)
-    float2 qa, qj;                      // error indicators (kVarStats): sum (m/r^2)^2, sum (m/r^3)^2
+    unsigned qa0, qa1, qj0, qj1;        // error indicators (kVarStats): bits of max m/(2r^2), max m/r^3
     double Ax, Ay, Az, Jx, Jy, Jz, Pt;
     float nr2;
     int nj, idx, i;
@@ -275,7 +275,7 @@ __device__ __forceinline__ void load_i(StateMixedP &s, const IRec &q, const Forc
     s.h2 = (float)q.h2;
     s.idx = q.index;
     s.ax = s.ay = s.az = s.jx = s.jy = s.jz = s.pm = make_float2(0.f, 0.f);
-    s.qa = s.qj = make_float2(0.f, 0.f);
+    s.qa0 = s.qa1 = s.qj0 = s.qj1 = 0u;
     s.Ax = s.Ay = s.Az = s.Jx = s.Jy = s.Jz = s.Pt = 0.0;
     s.nr2 = FLT_MAX;
     s.nj = -1;
@@ -349,11 +349,16 @@ __device__ __forceinline__ void interact_pair(StateMixedP &s, const JPairMixed &
     const float2 mr3 = __fmul2_rn(mr, r2inv);
     const float2 a3 = __fmul2_rn(__fmul2_rn(rv, dup(-0.75f)), r2inv);
     if (STATS) {
-        // the refinement's error indicators: mr3 = m / r^3 exactly (see
-        // above), so u r2 = (m / r^2)^2 and u = (m / r^3)^2 (self: m = 0)
-        const float2 u = __fmul2_rn(mr3, mr3);
-        s.qa = __ffma2_rn(u, r2, s.qa);
-        s.qj = __fadd2_rn(s.qj, u);
+        // The refinement's error indicators, the largest single terms:
+        // mr y = -m/(2 r^2) (y is -2/r, see above) and mr3 = m/r^3 (self:
+        // m = 0).  Non-positive (resp. non-negative) floats order like their
+        // bit patterns read as unsigned, so the maxima are integer maxima,
+        // off the FMA pipe.
+        const float2 t = __fmul2_rn(mr, y);
+        s.qa0 = max(s.qa0, __float_as_uint(t.x));
+        s.qa1 = max(s.qa1, __float_as_uint(t.y));
+        s.qj0 = max(s.qj0, __float_as_uint(mr3.x));
+        s.qj1 = max(s.qj1, __float_as_uint(mr3.y));
     }
     s.pm = __fadd2_rn(s.pm, mr);
     s.ax = __ffma2_rn(mr3, dx, s.ax);
@@ -421,8 +426,9 @@ constexpr int kVarUnroll4 = 2;
 constexpr int kVarG4 = 4;
 // 8 = potential only (paired mixed and FP64 layouts): the energy sweeps.
 constexpr int kVarPot = 8;
-// 16 = paired mixed layout: also accumulate the refinement's error
-// indicators (two FP32x2 sums, three instructions per pair of j).
+// 16 = paired mixed layout: also track the refinement's error indicators
+// (the largest single acc and jerk terms: one FP32x2 multiply and four
+// integer maxima per pair of j).
 constexpr int kVarStats = 16;
 
 // Consume one shared-memory tile: this thread's j are kbase + m*JL.
@@ -533,8 +539,8 @@ __device__ __forceinline__ void to_partial(const StateMixedP &s, Partial &q) {
     q.pot = s.Pt;
     q.nn_r2 = (double)s.nr2;
     q.nn_j = s.nj;
-    q.qa = s.qa.x + s.qa.y;
-    q.qj = s.qj.x + s.qj.y;
+    q.qa = -2.f * __uint_as_float(max(s.qa0, s.qa1));  // max m / r^2
+    q.qj = __uint_as_float(max(s.qj0, s.qj1));         // max m / r^3
 }
 __device__ __forceinline__ void to_partial(const StateF64 &s, Partial &q) {
     q.acc[0] = s.Ax; q.acc[1] = s.Ay; q.acc[2] = s.Az;
@@ -553,8 +559,8 @@ __device__ __forceinline__ void add_partial(Partial &a, const Partial &b) {
     }
     a.pot += b.pot;
     take_min(a.nn_r2, a.nn_j, b.nn_r2, b.nn_j);
-    a.qa += b.qa;
-    a.qj += b.qj;
+    a.qa = fmaxf(a.qa, b.qa);
+    a.qj = fmaxf(a.qj, b.qj);
 }
 
 // Sum over the lanes of a warp that share an i (lane bits >= log2(IL)).

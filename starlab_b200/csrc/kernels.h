@@ -250,8 +250,8 @@ void launch_split_finish(cudaStream_t s, int ni, int g, long long nj_total, cons
 
 // Mixed-mode FP64 refinement (refine.cu): particles whose error indicators
 // (ForceParams::out_q) exceed the bounds below are recomputed in FP64.
-constexpr double kRefineA = 1.0;  // sqrt(sum (m/r^2)^2) / |acc|
-constexpr double kRefineJ = 3.0;  // sqrt(sum (m/r^3)^2) v_rms / |jerk|
+constexpr double kRefineA = 1.0;  // max (m/r^2) / |acc|
+constexpr double kRefineJ = 1.6;  // max (m/r^3) v_rms / |jerk|
 constexpr int kRefineBlocks = 256;
 struct RefineArgs {
     int ni, nj, nj_pad, ident;

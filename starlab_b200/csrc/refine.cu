@@ -4,14 +4,15 @@
 // particle whose acceleration is the small remainder of large, nearly
 // cancelling terms -- one dominant neighbour or massive star against the
 // rest of the cluster -- then has a relative error of that size times the
-// ratio of the dominant terms to the total.  The paired kernel accumulates
-// two indicators per i, qa = sum (m/r^2)^2 and qj = sum (m/r^3)^2; measured
-// on the N = 262144 Plummer/Salpeter sweep against the FP64 engine, the
-// error of acc follows 2-6e-7 x sqrt(qa)/|a| and that of jerk 3-8e-7 x
-// sqrt(qj) v_rms/|jerk| (v_rms: rms speed of the j-set).  A particle is
-// flagged when sqrt(qa)/|a| > kRefineA or sqrt(qj) v_rms/|jerk| > kRefineJ
-// (about 1% of a Plummer sphere) and recomputed with the FP64 kernel against
-// FP64 j-records of the same block time; its results replace the mixed ones.
+// ratio of the dominant terms to the total.  The paired kernel tracks two
+// indicators per i, the largest single terms qa = max m/r^2 and qj = max
+// m/r^3; measured on the N = 262144 Plummer/Salpeter sweep against the FP64
+// engine, every particle whose acc error exceeds 0.4e-6 has qa/|a| >= 1.2
+// and every one whose jerk error exceeds 4e-6 has qj v_rms/|jerk| >= 2.0
+// (v_rms: rms speed of the j-set).  A particle is flagged when qa/|a| >
+// kRefineA or qj v_rms/|jerk| > kRefineJ (1-2% of a Plummer sphere) and
+// recomputed with the FP64 kernel against FP64 j-records of the same block
+// time; its results replace the mixed ones.
 // Everything stays on the device: flagging and compaction, the item of the
 // FP64 pass (its size read on the device by the batched kernel), the
 // scatter of the results.
@@ -71,7 +72,7 @@ __global__ void flag_kernel(int ni, const double *__restrict__ acc, const double
                       jerk[3 * (size_t)i + 2] * jerk[3 * (size_t)i + 2];
     const double qa = q[2 * (size_t)i], qj = q[2 * (size_t)i + 1];
     // flagged unless both ratios are finite and within their bounds
-    const bool good = qa <= kRefineA * kRefineA * a2 && qj * vrms * vrms <= kRefineJ * kRefineJ * j2;
+    const bool good = qa * qa <= kRefineA * kRefineA * a2 && qj * qj * vrms * vrms <= kRefineJ * kRefineJ * j2;
     if (good) return;
     const int k = atomicAdd(count, 1);
     list[k] = i;
