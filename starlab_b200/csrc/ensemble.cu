@@ -56,6 +56,7 @@ struct EnsDev {
     Partial *part;
     ForceParams *items;
     int *task0, *ipre, *counter;
+    int *order;  // [nc] clusters in task order (scan kernel)
     int *tcnt;  // per-particle slots of i-tile arrival counters (split reduction in the force kernel)
     unsigned *status;
     int *active;
@@ -181,13 +182,32 @@ __global__ void __launch_bounds__(1024) ens_scan_kernel(EnsDev d) {
     __shared__ int s_t[32], s_i[32], s_a[32];
     __shared__ unsigned long long s_x[32];
     const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+    // Task order: clusters by descending work per task (longest tasks first,
+    // so that the persistent CTAs' last tasks are short ones), ties by
+    // cluster number; clusters with no task last.
+    for (int c = tid; c < d.nc; c += 1024) {
+        auto key = [&](int q) -> long long {
+            if (d.ntask[q] == 0) return -1;
+            const ForceParams &p = d.items[q];
+            const int it = batch_item_itile(d.kmode, d.cfg, p.ni);
+            return (long long)min(it, p.ni) * p.jper;
+        };
+        const long long kc = key(c);
+        int rank = 0;
+        for (int q = 0; q < d.nc; ++q) {
+            const long long kq = key(q);
+            rank += kq > kc || (kq == kc && q < c);
+        }
+        d.order[rank] = c;
+    }
+    __syncthreads();
     const int per = (d.nc + 1023) / 1024;
     const int b = min(tid * per, d.nc), e = min(b + per, d.nc);
     int lt = 0, li = 0, la = 0;
     unsigned long long lx = 0;
     for (int c = b; c < e; ++c) {
         const int cnt = d.count[c];
-        lt += d.ntask[c];
+        lt += d.ntask[d.order[c]];  // tasks in the sorted order (position c)
         li += cnt;
         la += cnt > 0;
         lx += (unsigned long long)cnt * (unsigned long long)d.n[c];
@@ -225,9 +245,9 @@ __global__ void __launch_bounds__(1024) ens_scan_kernel(EnsDev d) {
     }
     int t = wt + it - lt, i2 = wi + ii - li;  // exclusive prefix of this thread's run
     for (int c = b; c < e; ++c) {
-        d.task0[c] = t;
-        d.ipre[c] = i2;
-        t += d.ntask[c];
+        d.task0[c] = t;  // prefix over the sorted order (position c)
+        d.ipre[c] = i2;  // prefix over the clusters
+        t += d.ntask[d.order[c]];
         i2 += d.count[c];
     }
     if (tid == 1023) {
@@ -571,6 +591,7 @@ int Ensemble::setup() {
     ECHK(alloc(&p, sizeof(int) * (nc_ + 1)), "alloc"); d_.task0 = (int *)p;
     ECHK(alloc(&p, sizeof(int) * (nc_ + 1)), "alloc"); d_.ipre = (int *)p;
     ECHK(alloc(&p, sizeof(int) * 4), "alloc"); d_.counter = (int *)p;
+    ECHK(alloc(&p, sizeof(int) * nc_), "alloc"); d_.order = (int *)p;
     ECHK(alloc(&p, sizeof(int) * N), "alloc"); d_.tcnt = (int *)p;
     ECHK(alloc(&p, sizeof(unsigned) * 4), "alloc"); d_.status = (unsigned *)p;
     ECHK(alloc(&p, sizeof(int) * 4), "alloc"); d_.active = (int *)p;
@@ -654,6 +675,7 @@ int Ensemble::iteration(int mode) {
     ba.H = d_.cfg.H;
     ba.counter = d_.counter;
     ba.one_task_per_cta = 0;
+    ba.order = d_.order;
     // total_i = 0: the splits are folded inside the force kernel (tile_counter)
     cudaError_t e = launch_force_batch(stream_, kmode_, d_.cfg, ba, ctas_, 0, false, true);
     if (e != cudaSuccess) return fail("force launch", e);

@@ -90,7 +90,7 @@ __global__ void __launch_bounds__(256, MinBlocks<K, R>::value) batch_force_kerne
             const int mid = (lo + hi + 1) >> 1;
             if (a.task0[mid] <= task) lo = mid; else hi = mid - 1;
         }
-        const ForceParams p = a.items[lo];
+        const ForceParams p = a.items[a.order ? a.order[lo] : lo];
         const int local = task - a.task0[lo];
         const int il = batch_il(p.ni);  // the item's lane shape (its H is in p.H)
         bool ok;

@@ -83,6 +83,9 @@ struct BatchArgs {
     int H;                     // j-subranges per CTA (same for every item)
     int *counter;              // task counter, zero before the launch
     int one_task_per_cta;      // 1: grid = tasks, CTA b runs task b (no counter)
+    // Optional [n_items]: task0 is a prefix over items[order[0]],
+    // items[order[1]], ... (the order tasks are handed out in); null = 0, 1, ...
+    const int *order = nullptr;
 };
 
 struct ForceConfig {
@@ -184,15 +187,15 @@ __host__ __device__ inline int batch_item_itile(int kmode, const ForceConfig &cf
 
 // Split rule of the batched kernel: a number of tasks wanted per item that
 // depends on the item alone (never on the batch): cfg.nsplit when set, e.g.
-// by the ensemble's tuner, else 592 = 4 x 148, but no more than one task per
-// kMinTaskWork interactions (small calls stay in few tasks, so a batch of
-// many calls is not cut into tasks too small to keep the pipeline busy), and
-// at least 4 tiles per split.
+// by the ensemble's tuner; else 592 = 4 x 148 but no more than one task per
+// kMinTaskWork interactions (the servers: small calls stay in few tasks, so
+// a batch of many calls is not cut into tasks too small to keep the
+// pipeline busy); at least 4 tiles per split.
 constexpr long long kMinTaskWork = 65536;
 __host__ __device__ inline void batch_plan(int kmode, const ForceConfig &cfg, ForceParams &item, int &n_tasks) {
     const long long work_cap = ((long long)item.ni * item.nj_pad) / kMinTaskWork;
-    const long long target = cfg.nsplit > 0 ? cfg.nsplit : 592;
-    const int kTargetTasks = (int)(work_cap < 1 ? 1 : (work_cap < target ? work_cap : target));
+    const int kTargetTasks = cfg.nsplit > 0 ? cfg.nsplit
+                                            : (int)(work_cap < 1 ? 1 : (work_cap < 592 ? work_cap : 592));
     const int T = tile_of(kmode);
     const int ntiles = item.nj_pad / T;
     const int itile = batch_item_itile(kmode, cfg, item.ni);
