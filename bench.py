@@ -187,6 +187,7 @@ def ensemble_section(nc, t_full, seed):
                            "interactions_per_s": st["interactions"] / st["seconds"],
                            "iterations": st["iterations"], "tuned_i_tile": 256 // st["tuned_h"],
                            "tuned_tasks_per_cluster": st["tuned_tasks"],
+                           "lane_efficiency": st["interactions"] / max(1, st["lane_interactions"]),
                            "dE_over_E_median": float(np.median(de)), "dE_over_E_max": float(de.max())}
     slice_t = 1.0 / 64
     for key, per in (("batched_slice", False), ("per_cluster_slice", True)):
@@ -507,6 +508,7 @@ def profile_ensemble(argv):
     e.close()
     st["interactions_per_s"] = st["interactions"] / st["seconds"]
     st["us_per_iteration"] = st["seconds"] / st["iterations"] * 1e6
+    st["lane_efficiency"] = st["interactions"] / max(1, st["lane_interactions"])
     print(json.dumps(st))
     return 0
 
@@ -588,8 +590,21 @@ def energy_drift(argv):
     return 0
 
 
+def serve(argv):
+    """The served-stream section alone (48 clusters, Poisson arrivals) at
+    the given rates; prints one JSON line."""
+    ap = argparse.ArgumentParser(prog="bench.py serve")
+    ap.add_argument("--rates", default="2000,20000")
+    ap.add_argument("--calls", type=int, default=3000)
+    ap.add_argument("--seed", type=int, default=5)
+    a = ap.parse_args(argv)
+    rates = tuple(float(r) for r in a.rates.split(","))
+    print(json.dumps(served_section(a.seed, rates=rates, n_calls=a.calls)), flush=True)
+    return 0
+
+
 SUB_MODES = {"profile-case": profile_case, "profile-ensemble": profile_ensemble, "profile-story": profile_story,
-             "energy-drift": energy_drift}
+             "energy-drift": energy_drift, "serve": serve}
 
 
 def main():

@@ -218,6 +218,9 @@ typedef struct {
     long long launches;
     int tuned_h;
     int tuned_tasks;     /* j-split factor chosen by the tuner (tasks wanted per cluster) */
+    long long lane_interactions; /* i-lanes x j-records the force kernel ran (whole i-tiles,
+                                  * j padded to its tile): interactions / lane_interactions is
+                                  * the share of the kernel's lanes doing useful pairs */
 } g6b200_ens_stats;
 g6b200_ensemble *g6b200_ens_create(int nclusters, const int *n, const double *eps2, double eta,
                                    int precision, int device);

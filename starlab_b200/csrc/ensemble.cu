@@ -8,18 +8,23 @@
 // j-state of every cluster stays in HBM.  One iteration advances EVERY
 // active cluster by its own next block:
 //
-//   schedule   one CTA per cluster: block time t_b = min(t_i + dt_i), the
-//              ordered list of block members, and the cluster's work item
-//              (a ForceParams: its j-records, i-records, softening,
-//              fixed-point scale, outputs, split plan)
-//   scan       prefix sums of the items' task and i counts
 //   predict    all particles of active clusters to their own t_b (FP64),
-//              j-records in the force kernel's layout, i-records of members
+//              j-records in the force kernel's layout; the block members
+//              (t_i + dt_i == t_b) compacted into i-records
+//   scan       each cluster's work item (a ForceParams: its j-records,
+//              i-records, softening, fixed-point scale, outputs, split
+//              plan), the task order, prefix sums of task and i counts
 //   force      ONE persistent launch over the (cluster, i-tile, j-split)
-//              work list of all clusters, then the split reduction
-//   correct    Hermite corrector in FP64 + new timestep, in place
+//              work list of all clusters, the splits folded in-kernel
+//   correct    Hermite corrector in FP64 + new timestep, in place; the
+//              next block time t_b = min(t_i + dt_i) of every cluster
+//              (members here, the others in predict), published by the
+//              corrector's last CTA
 //
-// The iteration is captured once as a CUDA graph and replayed.  For
+// The first block step of a run (and the start and energy sweeps) take
+// their block time and members from a schedule kernel instead (one CTA per
+// cluster, address order).  The steady-state iteration is captured once as
+// a CUDA graph and replayed.  For
 // comparison, run_per_cluster drives the same integration through the plain
 // single-cluster engine (one g6 firsthalf/lasthalf2 call per cluster per
 // block, host-side prediction and correction) -- the way independent kira
@@ -57,6 +62,8 @@ struct EnsDev {
     ForceParams *items;
     int *task0, *ipre, *counter;
     int *order;  // [nc] clusters in task order (scan kernel)
+    unsigned long long *tnext;  // [nc] next block time being formed (bits of a non-negative double; min)
+    unsigned *done;             // corrector CTAs finished (the last one publishes tnext)
     int *tcnt;  // per-particle slots of i-tile arrival counters (split reduction in the force kernel)
     unsigned *status;
     int *active;
@@ -84,6 +91,7 @@ __device__ __forceinline__ void predict_state(const EnsDev &d, int g, double tb,
 // all of a step's loads are issued before any of them is used, so a large
 // cluster keeps enough bytes in flight (the kernel is latency-bound
 // otherwise: one CTA walks up to 16384 particles).
+constexpr unsigned long long kTimeInf = 0x7ff0000000000000ull;  // bits of +inf (tnext: no time yet)
 constexpr int kSchedThreads = 512;
 constexpr int kSchedPer = 8;
 
@@ -149,68 +157,89 @@ __global__ void __launch_bounds__(kSchedThreads) ens_schedule_kernel(EnsDev d, i
         __syncthreads();
     }
     if (tid == 0) {
-        const int total = running;
-        d.count[c] = total;
+        d.count[c] = running;
         d.tblock[c] = tb;
-        ForceParams p{};
-        const size_t jb = d.kmode == kKernF64 ? sizeof(JRecF64) : sizeof(JRecMixed);
-        p.jrec = static_cast<const char *>(d.jrec) + (size_t)o * jb;
-        p.nj = n;
-        p.nj_pad = (n + tile_of(d.kmode) - 1) / tile_of(d.kmode) * tile_of(d.kmode);
-        p.irec = d.irec + o;
-        p.ni = total;
-        p.eps2 = d.eps2[c];
-        p.fs = d.fs[c];
-        p.part = d.part + d.part_off[c];
-        p.out_acc = d.acc1 + 3 * (size_t)o;
-        p.out_jerk = d.jerk1 + 3 * (size_t)o;
-        p.out_pot = d.pot1 + o;
-        p.out_nn = d.nn1 + o;
-        p.status = d.status;
-        p.tile_counter = d.tcnt + o;  // n_itiles <= ni <= n: the last CTA of an i-tile adds its splits
-        int nt = 0;
-        batch_plan(d.kmode, d.cfg, p, nt);
-        d.items[c] = p;
-        d.ntask[c] = nt;
+        d.tnext[c] = kTimeInf;
     }
+}
+
+// Work item of cluster c with ni block members.
+__device__ __forceinline__ void make_item(const EnsDev &d, int c, int ni, ForceParams &p, int &nt) {
+    const int o = d.off[c], n = d.n[c];
+    const size_t jb = d.kmode == kKernF64 ? sizeof(JRecF64) : sizeof(JRecMixed);
+    p = ForceParams{};
+    p.jrec = static_cast<const char *>(d.jrec) + (size_t)o * jb;
+    p.nj = n;
+    p.nj_pad = (n + tile_of(d.kmode) - 1) / tile_of(d.kmode) * tile_of(d.kmode);
+    p.irec = d.irec + o;
+    p.ni = ni;
+    p.eps2 = d.eps2[c];
+    p.fs = d.fs[c];
+    p.part = d.part + d.part_off[c];
+    p.out_acc = d.acc1 + 3 * (size_t)o;
+    p.out_jerk = d.jerk1 + 3 * (size_t)o;
+    p.out_pot = d.pot1 + o;
+    p.out_nn = d.nn1 + o;
+    p.status = d.status;
+    p.tile_counter = d.tcnt + o;  // n_itiles <= ni <= n: the last CTA of an i-tile adds its splits
+    nt = 0;
+    batch_plan(d.kmode, d.cfg, p, nt);
 }
 
 // Exclusive prefix sums of the clusters' task and member counts, the count
 // of active clusters and the interaction total: one CTA of 1024 threads,
 // each owning a contiguous run of clusters; warp-shuffle scans.
+constexpr int kOrderMax = 4096;  // clusters ordered by work per task (32 KB of keys)
+
 __global__ void __launch_bounds__(1024) ens_scan_kernel(EnsDev d) {
     __shared__ int s_t[32], s_i[32], s_a[32];
-    __shared__ unsigned long long s_x[32];
+    __shared__ unsigned long long s_x[32], s_l[32];
+    __shared__ long long s_key[kOrderMax];
     const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
     // Task order: clusters by descending work per task (longest tasks first,
     // so that the persistent CTAs' last tasks are short ones), ties by
-    // cluster number; clusters with no task last.
+    // cluster number; clusters with no task last.  Each key is computed once
+    // into shared memory and ranked by counting; above kOrderMax clusters the
+    // order is the cluster order.
     for (int c = tid; c < d.nc; c += 1024) {
-        auto key = [&](int q) -> long long {
-            if (d.ntask[q] == 0) return -1;
-            const ForceParams &p = d.items[q];
-            const int it = batch_item_itile(d.kmode, d.cfg, p.ni);
-            return (long long)min(it, p.ni) * p.jper;
-        };
-        const long long kc = key(c);
-        int rank = 0;
-        for (int q = 0; q < d.nc; ++q) {
-            const long long kq = key(q);
-            rank += kq > kc || (kq == kc && q < c);
+        ForceParams p;
+        int nt;
+        make_item(d, c, d.count[c], p, nt);
+        d.items[c] = p;
+        d.ntask[c] = nt;
+        if (c < kOrderMax) s_key[c] = nt > 0 ? (long long)min(batch_item_itile(d.kmode, d.cfg, p.ni), p.ni) * p.jper
+                                             : -1;
+    }
+    __syncthreads();
+    if (d.nc <= kOrderMax) {
+        for (int c = tid; c < d.nc; c += 1024) {
+            const long long kc = s_key[c];
+            int rank = 0;
+            for (int q = 0; q < d.nc; ++q) {
+                const long long kq = s_key[q];
+                rank += kq > kc || (kq == kc && q < c);
+            }
+            d.order[rank] = c;
         }
-        d.order[rank] = c;
+    } else {
+        for (int c = tid; c < d.nc; c += 1024) d.order[c] = c;
     }
     __syncthreads();
     const int per = (d.nc + 1023) / 1024;
     const int b = min(tid * per, d.nc), e = min(b + per, d.nc);
     int lt = 0, li = 0, la = 0;
-    unsigned long long lx = 0;
+    unsigned long long lx = 0, ll = 0;
     for (int c = b; c < e; ++c) {
         const int cnt = d.count[c];
         lt += d.ntask[d.order[c]];  // tasks in the sorted order (position c)
         li += cnt;
         la += cnt > 0;
         lx += (unsigned long long)cnt * (unsigned long long)d.n[c];
+        if (cnt > 0) {  // lanes the force kernel runs: whole i-tiles x padded j
+            const ForceParams &p = d.items[c];
+            const int it = batch_item_itile(d.kmode, d.cfg, cnt);
+            ll += (unsigned long long)((cnt + it - 1) / it * it) * (unsigned long long)p.nj_pad;
+        }
     }
     // inclusive warp scans of lt, li; warp sums of la, lx
     int it = lt, ii = li;
@@ -223,11 +252,12 @@ __global__ void __launch_bounds__(1024) ens_scan_kernel(EnsDev d) {
         }
     }
     int sa = la;
-    unsigned long long sx = lx;
+    unsigned long long sx = lx, sl = ll;
 #pragma unroll
     for (int k = 16; k > 0; k >>= 1) {
         sa += __shfl_xor_sync(0xffffffffu, sa, k);
         sx += __shfl_xor_sync(0xffffffffu, sx, k);
+        sl += __shfl_xor_sync(0xffffffffu, sl, k);
     }
     if (lane == 31) {
         s_t[w] = it;
@@ -236,6 +266,7 @@ __global__ void __launch_bounds__(1024) ens_scan_kernel(EnsDev d) {
     if (lane == 0) {
         s_a[w] = sa;
         s_x[w] = sx;
+        s_l[w] = sl;
     }
     __syncthreads();
     int wt = 0, wi = 0;
@@ -252,30 +283,74 @@ __global__ void __launch_bounds__(1024) ens_scan_kernel(EnsDev d) {
     }
     if (tid == 1023) {
         int act = 0;
-        unsigned long long inter = 0;
+        unsigned long long inter = 0, lanes = 0;
         for (int k = 0; k < 32; ++k) {
             act += s_a[k];
             inter += s_x[k];
+            lanes += s_l[k];
         }
         d.task0[d.nc] = t;
         d.ipre[d.nc] = i2;
         *d.active = act;
-        *d.interactions += inter;
+        d.interactions[0] += inter;
+        d.interactions[1] += lanes;
         *d.counter = 0;
     }
 }
 
 // Paired mixed records (one thread per pair) or FP64 records (one thread
 // per particle); i-records for the block members.
-__global__ void ens_predict_kernel(EnsDev d) {
+//
+// fused = 0: the members are those the schedule kernel listed (slot[]).
+// fused = 1 (block steps after the first of a run): the block time is the
+// one the previous corrector published, and the members -- t + dt equal to
+// it -- are compacted here: one atomic per warp on the cluster's count, the
+// warp's members in lane order after it.  The slot order then varies from
+// run to run; the forces do not (each i's sums are independent of its
+// slot).  Either way the non-members' t + dt go into the next block time
+// (tnext, a min over bit patterns of non-negative doubles); the corrector
+// adds the members' new t + dt.
+//
+// A warp never straddles two clusters (cluster spans are multiples of 256
+// particles), so its early returns are warp-uniform and the ballots below
+// see all 32 lanes.
+__global__ void ens_predict_kernel(EnsDev d, int fused) {
     const int per = d.kmode == kKernMixedP ? 2 : 1;
     const int q = blockIdx.x * blockDim.x + threadIdx.x;
     const int g0 = q * per;
     if (g0 >= d.ntot) return;
     const int c = d.cid[g0];
-    if (c < 0 || d.count[c] == 0) return;
+    if (c < 0) return;
     const int o = d.off[c], n = d.n[c];
     const double tb = d.tblock[c];
+    if (fused ? (n == 0 || !(tb <= d.t_end)) : d.count[c] == 0) return;  // inactive: tnext stays +inf
+    int sl[2] = {-1, -1};
+    unsigned long long tn_min = kTimeInf;
+    {
+        bool mem[2] = {false, false};
+        for (int u = 0; u < per; ++u) {
+            const int g = g0 + u, i = g - o;
+            if (i >= n) continue;
+            const double tn = d.t[g] + d.dt[g];
+            mem[u] = fused ? tn == tb : d.slot[g] >= 0;
+            if (!mem[u]) tn_min = min(tn_min, (unsigned long long)__double_as_longlong(tn));
+        }
+        if (fused) {
+            const unsigned lane = threadIdx.x & 31u, below = (1u << lane) - 1u;
+            const unsigned b0 = __ballot_sync(0xffffffffu, mem[0]), b1 = __ballot_sync(0xffffffffu, mem[1]);
+            const int tot = __popc(b0) + __popc(b1);
+            int base = 0;
+            if (lane == 0 && tot > 0) base = atomicAdd(&d.count[c], tot);
+            base = __shfl_sync(0xffffffffu, base, 0);
+            sl[0] = mem[0] ? base + __popc(b0 & below) : -1;
+            sl[1] = mem[1] ? base + __popc(b0) + __popc(b1 & below) : -1;
+            for (int u = 0; u < per; ++u) d.slot[g0 + u] = sl[u];
+        } else {
+            for (int u = 0; u < per; ++u) sl[u] = g0 + u - o < n ? d.slot[g0 + u] : -1;
+        }
+        for (int k = 16; k > 0; k >>= 1) tn_min = min(tn_min, __shfl_xor_sync(0xffffffffu, tn_min, k));
+        if ((threadIdx.x & 31u) == 0 && tn_min != kTimeInf) atomicMin(&d.tnext[c], tn_min);
+    }
     float hi[2][3], lo[2][3], vv[2][3], mm[2];
     int id[2];
     bool bad = false;
@@ -284,7 +359,7 @@ __global__ void ens_predict_kernel(EnsDev d) {
         if (i < n) {
             double xp[3], vp[3];
             predict_state(d, g, tb, xp, vp);
-            const int s = d.slot[g];
+            const int s = sl[u];
             if (s >= 0) {
                 IRec r;
                 for (int k = 0; k < 3; ++k) {
@@ -405,17 +480,55 @@ __device__ __forceinline__ void correct_one(const EnsDev &d, int mode, int c, in
 
 // Grid-stride over the block members only (ipre[nc] of them): member m is
 // slot s of cluster c, particle o + irec[o + s].index.
+// Each member's new t + dt goes into its cluster's tnext; the last CTA to
+// finish publishes tnext as the next block time (tblock), and resets tnext
+// and the member counts for the next iteration's predict kernel.
+//
+// Members are in cluster order, so a warp's lanes of one cluster are
+// contiguous: a segmented min over the warp leaves one atomic per cluster
+// per warp (the lane that heads the cluster's run).
 __global__ void ens_correct_kernel(EnsDev d, int mode) {
+    __shared__ bool s_last;
     const int total = d.ipre[d.nc];
-    for (int m = blockIdx.x * blockDim.x + threadIdx.x; m < total; m += gridDim.x * blockDim.x) {
-        int lo = 0, hi = d.nc - 1;
-        while (lo < hi) {
-            const int mid = (lo + hi + 1) >> 1;
-            if (d.ipre[mid] <= m) lo = mid; else hi = mid - 1;
+    const int lane = threadIdx.x & 31;
+    for (int m0 = blockIdx.x * blockDim.x; m0 < total; m0 += gridDim.x * blockDim.x) {  // block-uniform
+        const int m = m0 + threadIdx.x;
+        int c = -1;
+        unsigned long long tn = kTimeInf;
+        if (m < total) {
+            int lo = 0, hi = d.nc - 1;
+            while (lo < hi) {
+                const int mid = (lo + hi + 1) >> 1;
+                if (d.ipre[mid] <= m) lo = mid; else hi = mid - 1;
+            }
+            c = lo;
+            const int s = m - d.ipre[c], o = d.off[c];
+            const int g = o + d.irec[o + s].index;
+            correct_one(d, mode, c, o, s, g);
+            tn = (unsigned long long)__double_as_longlong(d.t[g] + d.dt[g]);
         }
-        const int c = lo, s = m - d.ipre[c], o = d.off[c];
-        correct_one(d, mode, c, o, s, o + d.irec[o + s].index);
+#pragma unroll
+        for (int k = 1; k < 32; k <<= 1) {
+            const unsigned long long ot = __shfl_down_sync(0xffffffffu, tn, k);
+            const int oc = __shfl_down_sync(0xffffffffu, c, k);
+            if (lane + k < 32 && oc == c) tn = min(tn, ot);
+        }
+        const int up = __shfl_up_sync(0xffffffffu, c, 1);
+        if (c >= 0 && (lane == 0 || up != c)) atomicMin(&d.tnext[c], tn);
     }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        s_last = atomicAdd(d.done, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!s_last) return;
+    __threadfence();
+    for (int c = threadIdx.x; c < d.nc; c += blockDim.x) {
+        d.tblock[c] = __longlong_as_double((long long)atomicExch(&d.tnext[c], kTimeInf));
+        d.count[c] = 0;
+    }
+    if (threadIdx.x == 0) *d.done = 0;
 }
 
 // Before a run: no step may jump over t_end, so every particle lands on it
@@ -468,6 +581,7 @@ struct EnsembleStats {
     long long launches = 0;
     double tuned_h = 0;
     int tuned_tasks = 0;
+    long long lane_interactions = 0;  // i-lanes x j the force kernel ran (whole i-tiles, padded j)
 };
 
 class Ensemble {
@@ -493,7 +607,8 @@ class Ensemble {
         return -1;
     }
     void release();
-    int iteration(int mode);  // schedule -> scan -> predict -> force -> correct
+    int iteration(int mode, bool fused = false);  // [schedule] -> predict -> scan -> force -> correct
+    long long launches_ = 0;  // kernels launched by iteration() (not counting graph captures)
     int sync_host_state();
     int push_host_state();
 
@@ -506,6 +621,7 @@ class Ensemble {
     int ntot_ = 0;
     long long max_iters_ = 2000000;  // run guards (G6B200_ENS_MAX_ITERS / _SECONDS)
     double max_seconds_ = 600.0;
+    bool fuse_ = true;  // G6B200_ENS_FUSED=0: every block step through the schedule kernel
     std::vector<int> off_;
     std::vector<double> hm_, hx_, hv_;  // host copies of the initial state
     EnsDev d_{};
@@ -537,6 +653,7 @@ void Ensemble::release() {
 int Ensemble::setup() {
     if (const char *e = getenv("G6B200_ENS_MAX_ITERS")) max_iters_ = atoll(e);
     if (const char *e = getenv("G6B200_ENS_MAX_SECONDS")) max_seconds_ = atof(e);
+    if (const char *e = getenv("G6B200_ENS_FUSED")) fuse_ = atoi(e) != 0;
     ECHK(cudaSetDevice(device_), "device");
     ECHK(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "stream");
     ECHK(cudaDeviceGetAttribute(&num_sms_, cudaDevAttrMultiProcessorCount, device_), "attr");
@@ -592,6 +709,8 @@ int Ensemble::setup() {
     ECHK(alloc(&p, sizeof(int) * (nc_ + 1)), "alloc"); d_.ipre = (int *)p;
     ECHK(alloc(&p, sizeof(int) * 4), "alloc"); d_.counter = (int *)p;
     ECHK(alloc(&p, sizeof(int) * nc_), "alloc"); d_.order = (int *)p;
+    ECHK(alloc(&p, sizeof(unsigned long long) * nc_), "alloc"); d_.tnext = (unsigned long long *)p;
+    ECHK(alloc(&p, sizeof(unsigned)), "alloc"); d_.done = (unsigned *)p;
     ECHK(alloc(&p, sizeof(int) * N), "alloc"); d_.tcnt = (int *)p;
     ECHK(alloc(&p, sizeof(unsigned) * 4), "alloc"); d_.status = (unsigned *)p;
     ECHK(alloc(&p, sizeof(int) * 4), "alloc"); d_.active = (int *)p;
@@ -657,16 +776,17 @@ int Ensemble::push_host_state() {
     return 0;
 }
 
-// Kernels launched by one iteration: schedule, scan, predict, force, and
-// (mode != 2) the corrector.
-constexpr int kLaunchesPerIteration = 5;
-
-int Ensemble::iteration(int mode) {
-    ens_schedule_kernel<<<nc_, kSchedThreads, 0, stream_>>>(d_, mode);
-    ens_scan_kernel<<<1, 1024, 0, stream_>>>(d_);
+// One iteration: schedule (unless fused), predict, scan, force and
+// (mode != 2) the corrector.  fused: block steps after the first of a run,
+// whose block times and members come from the previous corrector and the
+// predict kernel (mode 0 only).
+int Ensemble::iteration(int mode, bool fused) {
+    fused = fused && fuse_ && mode == 0;
+    if (!fused) ens_schedule_kernel<<<nc_, kSchedThreads, 0, stream_>>>(d_, mode);
     const int per = kmode_ == kKernMixedP ? 2 : 1;
     const int units = (ntot_ / per + 255) / 256;
-    ens_predict_kernel<<<units, 256, 0, stream_>>>(d_);
+    ens_predict_kernel<<<units, 256, 0, stream_>>>(d_, fused ? 1 : 0);
+    ens_scan_kernel<<<1, 1024, 0, stream_>>>(d_);
     BatchArgs ba;
     ba.items = d_.items;
     ba.task0 = d_.task0;
@@ -680,6 +800,7 @@ int Ensemble::iteration(int mode) {
     cudaError_t e = launch_force_batch(stream_, kmode_, d_.cfg, ba, ctas_, 0, false, true);
     if (e != cudaSuccess) return fail("force launch", e);
     if (mode != 2) ens_correct_kernel<<<4 * num_sms_, 256, 0, stream_>>>(d_, mode);
+    launches_ += (fused ? 3 : 4) + (mode != 2 ? 1 : 0);
     return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }
 
@@ -699,12 +820,17 @@ int Ensemble::run_batched(double t_end, EnsembleStats *st, int tune) {
         cudaGraphExecDestroy(graph_);
         graph_ = nullptr;
     }
-    unsigned long long i0 = 0;
+    unsigned long long i0 = 0, l0 = 0;
     ECHK(cudaMemcpy(&i0, d_.interactions, sizeof i0, cudaMemcpyDeviceToHost), "copy");
+    ECHK(cudaMemcpy(&l0, d_.interactions + 1, sizeof l0, cudaMemcpyDeviceToHost), "copy");
     ens_cap_kernel<<<(ntot_ + 255) / 256, 256, 0, stream_>>>(d_);
     ECHK(cudaStreamSynchronize(stream_), "cap");
     auto t0 = std::chrono::steady_clock::now();
-    long long iters = 0;
+    const long long launches0 = launches_;
+    // The run's first block step goes through the schedule kernel (the steps
+    // were capped at t_end since the last corrector); the rest are fused.
+    if (iteration(0, false)) return -1;
+    long long iters = 1;
     // Events and the pinned flag word are released on every return.
     struct Scratch {
         cudaEvent_t e0 = nullptr, e1 = nullptr;
@@ -734,7 +860,7 @@ int Ensemble::run_batched(double t_end, EnsembleStats *st, int tune) {
                 ctas_ = batch_ctas(kmode_, d_.cfg, num_sms_);
                 cudaEventRecord(e0, stream_);
                 for (int k = 0; k < 8; ++k)
-                    if (iteration(0)) return -1;
+                    if (iteration(0, true)) return -1;
                 cudaEventRecord(e1, stream_);
                 cudaEventSynchronize(e1);
                 iters += 8;
@@ -758,9 +884,12 @@ int Ensemble::run_batched(double t_end, EnsembleStats *st, int tune) {
     // Capture K iterations as one graph.
     const int K = 8;
     cudaGraph_t g;
+    const long long launches_before_capture = launches_;
     ECHK(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal), "capture");
-    for (int k = 0; k < K; ++k) iteration(0);
+    for (int k = 0; k < K; ++k) iteration(0, true);
     ECHK(cudaStreamEndCapture(stream_, &g), "capture");
+    const long long launches_per_graph = launches_ - launches_before_capture;
+    launches_ = launches_before_capture;
     ECHK(cudaGraphInstantiate(&graph_, g, 0), "instantiate");
     cudaGraphDestroy(g);
     // Two graph launches in flight: while the GPU runs one, the host waits
@@ -781,6 +910,7 @@ int Ensemble::run_batched(double t_end, EnsembleStats *st, int tune) {
     auto launch = [&](int slot) -> int {
         ECHK(cudaGraphLaunch(graph_, stream_), "graph launch");
         iters += K;
+        launches_ += launches_per_graph;
         ECHK(cudaMemcpyAsync(h_active + slot, d_.active, sizeof(int), cudaMemcpyDeviceToHost, stream_), "copy");
         ECHK(cudaEventRecord(done[slot], stream_), "event");
         return 0;
@@ -799,9 +929,10 @@ int Ensemble::run_batched(double t_end, EnsembleStats *st, int tune) {
     }
     ECHK(cudaStreamSynchronize(stream_), "run");
     auto t1 = std::chrono::steady_clock::now();
-    unsigned long long i1 = 0;
+    unsigned long long i1 = 0, l1 = 0;
     unsigned status = 0;
     ECHK(cudaMemcpy(&i1, d_.interactions, sizeof i1, cudaMemcpyDeviceToHost), "copy");
+    ECHK(cudaMemcpy(&l1, d_.interactions + 1, sizeof l1, cudaMemcpyDeviceToHost), "copy");
     ECHK(cudaMemcpy(&status, d_.status, sizeof status, cudaMemcpyDeviceToHost), "copy");
     if (status) {
         err = "ensemble: device status " + std::to_string(status) + " (fixed-point range or copy timeout)";
@@ -810,8 +941,9 @@ int Ensemble::run_batched(double t_end, EnsembleStats *st, int tune) {
     if (st) {
         st->seconds = std::chrono::duration<double>(t1 - t0).count();
         st->interactions = (long long)(i1 - i0);
+        st->lane_interactions = (long long)(l1 - l0);
         st->iterations = iters;
-        st->launches = iters * kLaunchesPerIteration;
+        st->launches = launches_ - launches0;
     }
     return 0;
 }
@@ -1066,6 +1198,7 @@ __attribute__((visibility("default"))) int g6b200_ens_run(g6b200_ensemble *h, do
         out->launches = st.launches;
         out->tuned_h = (int)st.tuned_h;
         out->tuned_tasks = st.tuned_tasks;
+        out->lane_interactions = st.lane_interactions;
     }
     return 0;
 }

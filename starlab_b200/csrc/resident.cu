@@ -274,21 +274,26 @@ __device__ int gather(const ResDev &d) {
     return n;
 }
 
+// One task of call k, i-lane shape IL.  Not inlined: each task body gets
+// its own register allocation (inlined beside the loop's other phases, the
+// shapes and self-test variants together spilled).
+template <int K, bool ID, int IL>
+__device__ __noinline__ bool run_task(const ForceParams *items, int k, int local, int itile, unsigned char *smem,
+                                      int &gt) {
+    const ForceParams p = items[k];
+    const int nit = (p.ni + itile - 1) / itile;
+    return process_task<K, IL, 1, false, ID, kVarUnroll4>(p, local % nit, local / nit, smem, gt);
+}
+
 template <int K, bool ID>
-__device__ __forceinline__ bool run_task(const ForceParams &p, int local, int itile, unsigned char *smem, int &gt) {
+__device__ __forceinline__ bool run_task_any(const ForceParams *items, int k, int local, unsigned char *smem,
+                                             int &gt) {
+    const ForceParams &p = items[k];
     const int il = batch_il(p.ni);
-    if (il == 32) {
-        const int nit = (p.ni + itile - 1) / itile;
-        return process_task<K, 32, 1, false, ID, kVarUnroll4>(p, local % nit, local / nit, smem, gt);
-    }
-    if (il == 8) {
-        const int it8 = (blockDim.x >> 5) / p.H * 8;
-        const int nit = (p.ni + it8 - 1) / it8;
-        return process_task<K, 8, 1, false, ID, kVarUnroll4>(p, local % nit, local / nit, smem, gt);
-    }
-    const int it1 = (blockDim.x >> 5) / p.H;
-    const int nit = (p.ni + it1 - 1) / it1;
-    return process_task<K, 1, 1, false, ID, kVarUnroll4>(p, local % nit, local / nit, smem, gt);
+    const int itile = (blockDim.x >> 5) / p.H * il;
+    if (il == 32) return run_task<K, ID, 32>(items, k, local, itile, smem, gt);
+    if (il == 8) return run_task<K, ID, 8>(items, k, local, itile, smem, gt);
+    return run_task<K, ID, 1>(items, k, local, itile, smem, gt);
 }
 
 template <int K>
@@ -300,7 +305,6 @@ __global__ void __launch_bounds__(256, 2) resident_kernel(const ResDev d) {
     if (threadIdx.x == 0) gen = atomicAdd(d.bar_gen, 0u);
     int gt = 0;
     bool failed = false;  // a grid barrier ran out
-    const int itile = (blockDim.x >> 5) / d.cfg.H * 32;
     for (;;) {
         // ---- gather
         if (blockIdx.x == 0) {
@@ -359,10 +363,9 @@ __global__ void __launch_bounds__(256, 2) resident_kernel(const ResDev d) {
             const int task = s_task;
             if (task >= total) break;
             const int k = find_item(d.task0, n, task);
-            ForceParams p = d.items[k];
             const int local = task - d.task0[k];
-            const bool ok = d.info[k].c.ident ? run_task<K, true>(p, local, itile, smem, gt)
-                                              : run_task<K, false>(p, local, itile, smem, gt);
+            const bool ok = d.info[k].c.ident ? run_task_any<K, true>(d.items, k, local, smem, gt)
+                                              : run_task_any<K, false>(d.items, k, local, smem, gt);
             if (!ok) {
                 // a copy wait ran out (the call's status says so): this CTA
                 // takes no further task, and the loop ends after this batch
@@ -437,6 +440,88 @@ double now_s() {
 
 }  // namespace
 
+// Pinned, mapped host memory for the requests' i-records and results.
+// Chunks are taken with cudaHostAlloc as needed and given back only at
+// shutdown: cudaFreeHost synchronises with the device, so freeing while the
+// resident kernel runs would stall the caller until the kernel's idle exit.
+// Inside a chunk, first fit over an offset-ordered free list, coalesced on
+// release.  Called with the server's mutex held.
+class PinnedArena {
+  public:
+    static constexpr size_t kAlign = 256;
+    static constexpr size_t kChunk = 64u << 20;
+
+    unsigned char *alloc(size_t bytes) {
+        bytes = std::max(kAlign, (bytes + kAlign - 1) / kAlign * kAlign);
+        for (Chunk &c : chunks_)
+            for (auto it = c.free.begin(); it != c.free.end(); ++it)
+                if (it->second >= bytes) {
+                    const size_t off = it->first, len = it->second;
+                    c.free.erase(it);
+                    if (len > bytes) c.free[off + bytes] = len - bytes;
+                    return c.base + off;
+                }
+        Chunk c;
+        c.size = std::max(kChunk, (bytes + (2u << 20) - 1) / (2u << 20) * (2u << 20));
+        void *q = nullptr;
+        if (cudaHostAlloc(&q, c.size, cudaHostAllocMapped) != cudaSuccess) return nullptr;
+        c.base = static_cast<unsigned char *>(q);
+        void *dq = nullptr;
+        if (cudaHostGetDevicePointer(&dq, q, 0) != cudaSuccess) {
+            cudaFreeHost(q);
+            return nullptr;
+        }
+        c.dbase = static_cast<unsigned char *>(dq);
+        if (c.size > bytes) c.free[bytes] = c.size - bytes;
+        chunks_.push_back(std::move(c));
+        return chunks_.back().base;
+    }
+
+    void release(unsigned char *p, size_t bytes) {
+        if (!p) return;
+        bytes = std::max(kAlign, (bytes + kAlign - 1) / kAlign * kAlign);
+        for (Chunk &c : chunks_) {
+            if (p < c.base || p >= c.base + c.size) continue;
+            size_t off = (size_t)(p - c.base), len = bytes;
+            auto nx = c.free.lower_bound(off);
+            if (nx != c.free.end() && off + len == nx->first) {
+                len += nx->second;
+                nx = c.free.erase(nx);
+            }
+            if (nx != c.free.begin()) {
+                auto pv = std::prev(nx);
+                if (pv->first + pv->second == off) {
+                    off = pv->first;
+                    len += pv->second;
+                    c.free.erase(pv);
+                }
+            }
+            c.free[off] = len;
+            return;
+        }
+    }
+
+    // The device's address of host address p (inside a chunk).
+    unsigned char *device_ptr(unsigned char *p) const {
+        for (const Chunk &c : chunks_)
+            if (p >= c.base && p < c.base + c.size) return c.dbase + (p - c.base);
+        return nullptr;
+    }
+
+    void destroy() {
+        for (Chunk &c : chunks_) cudaFreeHost(c.base);
+        chunks_.clear();
+    }
+
+  private:
+    struct Chunk {
+        unsigned char *base = nullptr, *dbase = nullptr;  // host and device addresses
+        size_t size = 0;
+        std::map<size_t, size_t> free;  // offset -> length
+    };
+    std::vector<Chunk> chunks_;
+};
+
 struct ResStats {
     long long batches = 0, calls = 0, launches = 0, recoveries = 0;
     int max_batch = 0;
@@ -485,9 +570,10 @@ class Resident {
         int inflight = 0;
     };
     struct SlotHost {
-        IRec *irec = nullptr;          // pinned, mapped
-        unsigned char *out = nullptr;  // pinned, mapped
-        size_t cap = 0;                // i-records the buffers hold
+        unsigned char *buf = nullptr;  // pinned, mapped (from arena_): i-records, then the results
+        size_t bytes = 0;
+        IRec *irec = nullptr;
+        unsigned char *out = nullptr;
         double t_submit = 0;
         int cluster = -1;
         long long id = -1;
@@ -518,6 +604,7 @@ class Resident {
     ResCtl *ctl_ = nullptr;       // pinned, mapped
     ResCluster *ctab_ = nullptr;  // pinned, mapped; one entry per cluster id
     SlotHost host_[kResSlots];
+    PinnedArena arena_;
     long long head_ = 0;  // next ring position to fill
     std::vector<long long> held_;
     bool holding_ = false;
@@ -631,11 +718,8 @@ void Resident::shutdown() {
         cudaFreeHost(c.h_index);
     }
     clusters_.clear();
-    for (SlotHost &s : host_) {
-        if (s.irec) cudaFreeHost(s.irec);
-        if (s.out) cudaFreeHost(s.out);
-        s = SlotHost();
-    }
+    for (SlotHost &s : host_) s = SlotHost();
+    arena_.destroy();
     cudaFreeHost(slots_);
     cudaFreeHost(ctl_);
     cudaFreeHost(ctab_);
@@ -776,21 +860,16 @@ long long Resident::submit(int c, double ti, int nj, int ni, const int *index, c
         return -1;
     }
     SlotHost &h = host_[k];
-    if ((size_t)ni > h.cap) {
-        if (h.irec) cudaFreeHost(h.irec);
-        if (h.out) cudaFreeHost(h.out);
-        h.irec = nullptr;
-        h.out = nullptr;
-        h.cap = 0;
-        const size_t cap = std::max<size_t>(ni, 256);
-        if (cudaHostAlloc(reinterpret_cast<void **>(&h.irec), sizeof(IRec) * cap, cudaHostAllocMapped) !=
-                cudaSuccess ||
-            cudaHostAlloc(reinterpret_cast<void **>(&h.out), 60 * cap, cudaHostAllocMapped) != cudaSuccess) {
-            err = "resident: pinned request buffers";
-            return -1;
-        }
-        h.cap = cap;
+    const size_t ibytes = sizeof(IRec) * (size_t)ni;
+    h.bytes = ibytes + 60 * (size_t)ni;
+    h.buf = arena_.alloc(h.bytes);
+    if (!h.buf) {
+        err = "resident: pinned request buffers";
+        return -1;
     }
+    h.irec = reinterpret_cast<IRec *>(h.buf);
+    h.out = h.buf + ibytes;
+    unsigned char *dbuf = arena_.device_ptr(h.buf);
     ++head_;
     double xm = cl.xmax;
     for (int i = 0; i < ni; ++i) {
@@ -815,15 +894,8 @@ long long Resident::submit(int c, double ti, int nj, int ni, const int *index, c
     s.ti = ti;
     s.eps2 = cl.eps2;
     s.fs = scale_of(cl.E);
-    IRec *di = nullptr;
-    unsigned char *dout = nullptr;
-    if (cudaHostGetDevicePointer(reinterpret_cast<void **>(&di), h.irec, 0) != cudaSuccess ||
-        cudaHostGetDevicePointer(reinterpret_cast<void **>(&dout), h.out, 0) != cudaSuccess) {
-        err = "resident: mapping";
-        return -1;
-    }
-    s.irec = di;
-    s.out = dout;
+    s.irec = reinterpret_cast<IRec *>(dbuf);
+    s.out = dbuf + ibytes;
     s.batch = -1;
     s.batch_size = 0;
     s.status = 0;
@@ -969,6 +1041,8 @@ int Resident::wait(long long id, double (*acc)[3], double (*jerk)[3], double *po
             if (rc == 4) it->second->E += 2;  // a wider grid for the caller's next submit
         }
         h.id = -1;
+        arena_.release(h.buf, h.bytes);
+        h.buf = nullptr;
         __atomic_store_n(&s.state, (int)kFree, __ATOMIC_RELEASE);
     }
     cv_idle_.notify_all();

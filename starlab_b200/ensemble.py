@@ -16,7 +16,7 @@ from .g6 import G6Error, load_library, _PREC
 class EnsStats(ctypes.Structure):
     _fields_ = [("seconds", ctypes.c_double), ("interactions", ctypes.c_longlong),
                 ("iterations", ctypes.c_longlong), ("launches", ctypes.c_longlong), ("tuned_h", ctypes.c_int),
-                ("tuned_tasks", ctypes.c_int)]
+                ("tuned_tasks", ctypes.c_int), ("lane_interactions", ctypes.c_longlong)]
 
 
 def _bind(lib):

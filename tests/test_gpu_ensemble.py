@@ -3,6 +3,9 @@
 * forces at t = 0 of every cluster against the FP64 oracle;
 * a cluster integrated alone and inside a mix of other clusters follows a
   bit-identical trajectory (its work items never depend on the others);
+* block steps scheduled inside the predict kernel and the corrector (the
+  steady state) and block steps through the schedule kernel give
+  bit-identical states;
 * the batched path and the plain one-call-per-cluster path agree, and both
   conserve energy (4th-order Hermite, eta = 0.02, t = 1/8).
 """
@@ -60,6 +63,27 @@ def test_alone_and_in_the_mix_are_bit_identical():
     assert np.all(a["t"] == 1.0 / 32)
     mix.close()
     alone.close()
+
+
+def test_fused_schedule_matches_the_schedule_kernel(monkeypatch):
+    """Block steps whose members and block time come from the previous
+    corrector and the predict kernel (atomic slot order) give bit-identical
+    states to block steps through the schedule kernel (address order)."""
+    cl = clusters([700, 1500, 256, 3000, 900], 31)
+    out = []
+    for fused in ("1", "0"):
+        monkeypatch.setenv("G6B200_ENS_FUSED", fused)
+        e = make(cl)
+        e.start()
+        st = e.run(1.0 / 32, tune=False)
+        out.append((st, [e.get(c) for c in range(len(cl))]))
+        e.close()
+    (s1, a), (s0, b) = out
+    assert s1["interactions"] == s0["interactions"] and s1["iterations"] == s0["iterations"]
+    assert s1["launches"] < s0["launches"]
+    for c in range(len(cl)):
+        for k in ("x", "v", "acc", "jerk", "t", "dt"):
+            assert np.array_equal(a[c][k], b[c][k]), (c, k)
 
 
 def test_batched_and_per_cluster_agree_and_conserve_energy():
