@@ -60,7 +60,7 @@ namespace storyk {
 
 constexpr int kLineMax = 254;  // get_line keeps 254 characters (MAX_INPUT_LINE_LENGTH 255)
 constexpr int kMaxDepth = 32;  // bracket nesting supported
-constexpr int kChunk = 64;     // lines per thread in the enclosing-line pass
+constexpr int kChunk = 32;     // lines per thread in the enclosing-line pass
 constexpr int kScanTile = 4096;
 constexpr int kNlThreads = 256, kNlBytes = 64, kNlTile = kNlThreads * kNlBytes;
 
@@ -73,7 +73,7 @@ enum : int { FLD_M = 0, FLD_R, FLD_V, FLD_TIME, FLD_I, FLD_NAME, FLD_COUNT };
 // Error codes (low byte of the error word; the line number above it).
 enum : int {
     E_NUL = 1, E_INDENT, E_TOP, E_CLOSE0, E_DEPTH, E_EOF, E_KIND, E_TITLE, E_CONFLICT, E_LONG, E_EMPTY,
-    E_KEYWORD, E_VECTOR, E_NUMBER
+    E_KEYWORD, E_VECTOR, E_NUMBER, E_SCAN
 };
 __host__ const char *error_text(int code) {
     switch (code) {
@@ -91,6 +91,7 @@ __host__ const char *error_text(int code) {
         case E_KEYWORD: return "unexpected keyword in a Particle";
         case E_VECTOR: return "expected three reals";
         case E_NUMBER: return "number form not supported (hexadecimal, NaN payload or more than 40 digits)";
+        case E_SCAN: return "internal: a device scan's wait for an earlier tile timed out";
         default: return "parse error";
     }
 }
@@ -184,19 +185,7 @@ __device__ __forceinline__ int block_excl_max(int v) {
     return r;
 }
 
-// Generic exclusive sum over n elements given by f(k): tile sums, a scan of
-// the tile sums in one block, then each tile scanned with its offset.
-template <class F>
-__global__ void __launch_bounds__(256) tile_sum_kernel(F f, long long n, int *tile_sum) {
-    const long long base = (long long)blockIdx.x * kScanTile + threadIdx.x * 16;
-    int s = 0;
-    for (int j = 0; j < 16; ++j)
-        if (base + j < n) s += f(base + j);
-    int tot;
-    block_excl_sum<256>(s, &tot);
-    if (threadIdx.x == 0) tile_sum[blockIdx.x] = tot;
-}
-
+// Exclusive sum of n values in one block (the newline index's block counts).
 template <class T>
 __global__ void __launch_bounds__(1024) scan_tiles_kernel(T *v, int n, T *total) {
     const int per = (n + 1023) / 1024;
@@ -213,62 +202,147 @@ __global__ void __launch_bounds__(1024) scan_tiles_kernel(T *v, int n, T *total)
     if (threadIdx.x == 0 && total) *total = tot;
 }
 
+// Single-pass exclusive sum (decoupled look-back): each CTA takes the next
+// tile by ticket (so every tile it waits for belongs to a CTA already
+// running), publishes its own sum, then walks back over the earlier tiles'
+// published sums until one carries its inclusive prefix.  A status word is
+// value | flag << 32 | epoch << 34; the epoch (one per scan) tells this
+// scan's words from an earlier scan's.  Waits are bounded: after kScanWaitNs
+// the scan reports E_SCAN and goes on.
+constexpr unsigned long long kScanWaitNs = 1000000000ull;
+enum : unsigned { SCAN_AGG = 1, SCAN_PREFIX = 2 };
+
+__device__ __forceinline__ unsigned long long story_clock_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
 template <class F>
-__global__ void __launch_bounds__(256) tile_apply_kernel(F f, long long n, const int *tile_off, int *out) {
-    const long long base = (long long)blockIdx.x * kScanTile + threadIdx.x * 16;
-    int v[16], s = 0;
-    for (int j = 0; j < 16; ++j) {
-        v[j] = base + j < n ? f(base + j) : 0;
-        s += v[j];
+__global__ void __launch_bounds__(256) scan1_kernel(F f, long long n, int *out, int *total,
+                                                    unsigned long long *status, unsigned long long *ticket,
+                                                    unsigned long long base, unsigned epoch, int ntiles,
+                                                    unsigned long long *err) {
+    __shared__ int s_tile, s_prefix;
+    if (threadIdx.x == 0) s_tile = (int)(atomicAdd(ticket, 1ull) - base);
+    __syncthreads();
+    const int tile = s_tile;
+    if (tile < 0 || tile >= ntiles) {  // tickets out of step with the host's count: report, write nothing
+        if (threadIdx.x == 0) report(err, 0, E_SCAN);
+        return;
     }
-    int run = block_excl_sum<256>(s, (int *)nullptr) + tile_off[blockIdx.x];
-    for (int j = 0; j < 16; ++j)
-        if (base + j < n) {
-            out[base + j] = run;
-            run += v[j];
+    // f is evaluated striped (element b + j * 256 + thread: coalesced), the
+    // values pass through shared memory to this thread's 16 consecutive
+    // elements (padded rows: one word per 32), and the results go back out
+    // striped.
+    __shared__ int sv[kScanTile + kScanTile / 32];
+    const long long b = (long long)tile * kScanTile;
+#pragma unroll
+    for (int j = 0; j < 16; ++j) {
+        const int i = j * 256 + threadIdx.x;
+        sv[i + i / 32] = b + i < n ? f(b + i) : 0;
+    }
+    __syncthreads();
+    int v[16], sum = 0;
+#pragma unroll
+    for (int j = 0; j < 16; ++j) {
+        const int i = threadIdx.x * 16 + j;
+        v[j] = sv[i + i / 32];
+        sum += v[j];
+    }
+    int agg;
+    const int excl = block_excl_sum<256>(sum, &agg);
+    if (threadIdx.x == 0) {
+        const unsigned long long ep = (unsigned long long)epoch << 34;
+        int prefix = 0;
+        if (tile > 0) {
+            atomicExch(&status[tile], ep | ((unsigned long long)SCAN_AGG << 32) | (unsigned)agg);
+            const unsigned long long t0 = story_clock_ns();
+            bool late = false;
+            for (int k = tile - 1; k >= 0;) {
+                const unsigned long long w = atomicAdd(&status[k], 0ull);
+                const unsigned fl = (unsigned)(w >> 32) & 3u;
+                if ((w >> 34) != (unsigned long long)epoch || fl == 0) {
+                    if (story_clock_ns() - t0 > kScanWaitNs) {
+                        late = true;
+                        break;
+                    }
+                    continue;
+                }
+                prefix += (int)(unsigned)w;
+                if (fl == SCAN_PREFIX) break;
+                --k;
+            }
+            if (late) report(err, 0, E_SCAN);
         }
+        atomicExch(&status[tile], ep | ((unsigned long long)SCAN_PREFIX << 32) | (unsigned)(prefix + agg));
+        if (tile == ntiles - 1 && total) *total = prefix + agg;
+        s_prefix = prefix;
+    }
+    __syncthreads();
+    int run = s_prefix + excl;
+#pragma unroll
+    for (int j = 0; j < 16; ++j) {
+        const int i = threadIdx.x * 16 + j;
+        sv[i + i / 32] = run;
+        run += v[j];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int j = 0; j < 16; ++j) {
+        const int i = j * 256 + threadIdx.x;
+        if (b + i < n) out[b + i] = sv[i + i / 32];
+    }
 }
 
 // ---------------------------------------------------------------------------
 // 1. Newline index.
 
-__device__ __forceinline__ void scan16(uint4 q, int valid, int &nl, bool &nul) {
-    const uint32_t w[4] = {q.x, q.y, q.z, q.w};
-#pragma unroll
-    for (int i = 0; i < 4; ++i) {
-        const int vb = min(max(valid - 4 * i, 0), 4);
-        const uint32_t keep = vb >= 4 ? 0xffffffffu : ((1u << (8 * vb)) - 1u);
-        nl += __popc(__vcmpeq4(w[i], 0x0a0a0a0au) & keep) >> 3;
-        nul |= (__vcmpeq4(w[i], 0u) & keep) != 0u;
-    }
+// A block covers kNlTile bytes as kNlBytes / 16 rounds of 16-byte chunks:
+// in round r thread t takes chunk r * kNlThreads + t (consecutive threads,
+// consecutive chunks: coalesced).  Bytes past len read as zero.
+__device__ __forceinline__ uint4 load16(const char *text, long long len, long long a) {
+    if (a + 16 <= len) return *reinterpret_cast<const uint4 *>(text + a);
+    uint32_t x[4] = {0, 0, 0, 0};
+    for (int b = 0; b < 16; ++b)
+        if (a + b < len) x[b >> 2] |= (uint32_t)(unsigned char)text[a + b] << (8 * (b & 3));
+    return make_uint4(x[0], x[1], x[2], x[3]);
 }
 
-__device__ __forceinline__ int valid16(long long left) { return left >= 16 ? 16 : (left <= 0 ? 0 : (int)left); }
-
-// The 64 bytes of one thread: 16-byte loads inside the text, single bytes
-// for the last partial segment (nothing past len is read).
-__device__ __forceinline__ void load64(const char *text, long long len, long long base, uint4 *q) {
-    if (base + kNlBytes <= len) {
-        const uint4 *p = reinterpret_cast<const uint4 *>(text + base);
-        for (int i = 0; i < 4; ++i) q[i] = p[i];
-        return;
+// Newline bits (bit b: byte b is '\n') and whether a NUL byte is present,
+// for the 16 bytes of a chunk ending `left` bytes before len.
+__device__ __forceinline__ uint32_t nl_bits16(uint4 q, long long left, bool &nul) {
+    const uint32_t w[4] = {q.x, q.y, q.z, q.w};
+    uint32_t bits = 0, zero = 0;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const uint32_t m = __vcmpeq4(w[k], 0x0a0a0a0au), z = __vcmpeq4(w[k], 0u);
+        bits |= (((m >> 7) & 1u) | ((m >> 14) & 2u) | ((m >> 21) & 4u) | ((m >> 28) & 8u)) << (4 * k);
+        zero |= (((z >> 7) & 1u) | ((z >> 14) & 2u) | ((z >> 21) & 4u) | ((z >> 28) & 8u)) << (4 * k);
     }
-    uint32_t w[16];
-    for (int j = 0; j < 16; ++j) w[j] = 0;
-    for (int b = 0; b < kNlBytes && base + b < len; ++b)
-        w[b >> 2] |= (uint32_t)(unsigned char)text[base + b] << (8 * (b & 3));
-    for (int i = 0; i < 4; ++i) q[i] = make_uint4(w[4 * i], w[4 * i + 1], w[4 * i + 2], w[4 * i + 3]);
+    const uint32_t keep = left >= 16 ? 0xffffu : (left <= 0 ? 0u : (1u << left) - 1u);
+    nul |= (zero & keep) != 0;
+    return bits & keep;
 }
 
 __global__ void __launch_bounds__(kNlThreads) nl_count_kernel(const char *text, long long len, long long *blk,
                                                               unsigned long long *err) {
-    const long long base = (long long)blockIdx.x * kNlTile + threadIdx.x * kNlBytes;
+    const long long base = (long long)blockIdx.x * kNlTile;
     int nl = 0;
     bool nul = false;
-    if (base < len) {
-        uint4 q[4];
-        load64(text, len, base, q);
-        for (int i = 0; i < 4; ++i) scan16(q[i], valid16(len - base - 16 * i), nl, nul);
+    uint4 q[kNlBytes / 16];
+    if (base + kNlTile <= len) {  // all loads in flight before any is used
+#pragma unroll
+        for (int r = 0; r < kNlBytes / 16; ++r)
+            q[r] = *reinterpret_cast<const uint4 *>(text + base + 16LL * (r * kNlThreads + threadIdx.x));
+    } else {
+#pragma unroll
+        for (int r = 0; r < kNlBytes / 16; ++r) q[r] = load16(text, len, base + 16LL * (r * kNlThreads + threadIdx.x));
+    }
+#pragma unroll
+    for (int r = 0; r < kNlBytes / 16; ++r) {
+        const long long a = base + 16LL * (r * kNlThreads + threadIdx.x);
+        if (a < len) nl += __popc(nl_bits16(q[r], len - a, nul));
     }
     if (nul) report(err, 0, E_NUL);
     int tot;
@@ -278,23 +352,29 @@ __global__ void __launch_bounds__(kNlThreads) nl_count_kernel(const char *text, 
 
 __global__ void __launch_bounds__(kNlThreads) nl_write_kernel(const char *text, long long len,
                                                               const long long *blk_off, long long *nl_pos) {
-    const long long base = (long long)blockIdx.x * kNlTile + threadIdx.x * kNlBytes;
-    int nl = 0;
+    const long long base = (long long)blockIdx.x * kNlTile;
+    long long o = blk_off[blockIdx.x];
     bool nul = false;
-    uint4 q[4];
-    if (base < len) {
-        load64(text, len, base, q);
-        for (int i = 0; i < 4; ++i) scan16(q[i], valid16(len - base - 16 * i), nl, nul);
+    uint4 q[kNlBytes / 16];
+    if (base + kNlTile <= len) {
+#pragma unroll
+        for (int r = 0; r < kNlBytes / 16; ++r)
+            q[r] = *reinterpret_cast<const uint4 *>(text + base + 16LL * (r * kNlThreads + threadIdx.x));
+    } else {
+#pragma unroll
+        for (int r = 0; r < kNlBytes / 16; ++r) q[r] = load16(text, len, base + 16LL * (r * kNlThreads + threadIdx.x));
     }
-    long long o = block_excl_sum<kNlThreads>(nl, (int *)nullptr) + blk_off[blockIdx.x];
-    if (nl == 0) return;
-    for (int i = 0; i < 4; ++i) {
-        const uint32_t w[4] = {q[i].x, q[i].y, q[i].z, q[i].w};
-        for (int j = 0; j < 16; ++j) {
-            const long long pos = base + 16 * i + j;
-            if (pos >= len) return;
-            if (((w[j >> 2] >> (8 * (j & 3))) & 0xffu) == '\n') nl_pos[o++] = pos;
+#pragma unroll
+    for (int r = 0; r < kNlBytes / 16; ++r) {
+        const long long a = base + 16LL * (r * kNlThreads + threadIdx.x);
+        uint32_t bits = a < len ? nl_bits16(q[r], len - a, nul) : 0u;
+        int tot;
+        long long at = o + block_excl_sum<kNlThreads>(__popc(bits), &tot);
+        while (bits) {
+            nl_pos[at++] = a + (__ffs(bits) - 1);
+            bits &= bits - 1;
         }
+        o += tot;
     }
 }
 
@@ -431,22 +511,40 @@ __global__ void check_kernel(const uint32_t *tag, const int *depth, const int *c
 
 // Blocks of kChunkThreads chunks: each chunk's last open line per level,
 // and the block's maximum per level (blk) for the scan across blocks.
+// The block's lines are staged in shared memory by coalesced loads, stored
+// chunk-transposed (line j of chunk c at j * kStageCols + c, kStageCols odd)
+// so that the 32 threads of a warp, walking their chunks in step, read 32
+// different banks.
 constexpr int kChunkThreads = 128;
+constexpr int kStageCols = kChunkThreads + 1;
+
+__device__ __forceinline__ int staged(int i) { return (i % kChunk) * kStageCols + i / kChunk; }
 
 __global__ void __launch_bounds__(kChunkThreads) chunk_last_kernel(const uint32_t *tag, const int *depth,
                                                                    const int *meta, int nchunks, int *sum, int *blk) {
     __shared__ int red[kChunkThreads / 32];
+    __shared__ uint32_t s_tag[kChunk * kStageCols];
+    __shared__ int s_dep[kChunk * kStageCols];
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     const int end = meta[0], L = meta[1];
+    const int b0 = blockIdx.x * kChunkThreads * kChunk;
+    const int cnt = max(0, min(end - b0, kChunkThreads * kChunk));
+    for (int i = threadIdx.x; i < cnt; i += kChunkThreads) {
+        s_tag[staged(i)] = tag[b0 + i];
+        s_dep[staged(i)] = depth[b0 + i];
+    }
+    __syncthreads();
     int last[kMaxDepth];
     for (int l = 0; l < L; ++l) last[l] = -1;
     if (c < nchunks) {
         const int b = c * kChunk, e = min(end, b + kChunk);
-        for (int k = b; k < e; ++k)
-            if (code_of(tag[k]) == C_OPEN) {
-                const int lv = depth[k] + 1;  // level of this open line (below 1 only in malformed text)
+        for (int k = b; k < e; ++k) {
+            const int i = staged(k - b0);
+            if (code_of(s_tag[i]) == C_OPEN) {
+                const int lv = s_dep[i] + 1;  // level of this open line (below 1 only in malformed text)
                 if (lv >= 1 && lv <= kMaxDepth) last[lv - 1] = k;
             }
+        }
         for (int l = 0; l < L; ++l) sum[(long long)c * kMaxDepth + l] = last[l];
     }
     for (int l = 0; l < L; ++l) {
@@ -481,32 +579,42 @@ __global__ void __launch_bounds__(1024) chunk_scan_kernel(int *sum, int nchunks,
 
 // blk holds, per block and level, the last open line before the block (an
 // exclusive scan of chunk_last_kernel's maxima); the chunks of the block
-// scan their own maxima to get the open lines around their start.
+// scan their own maxima to get the open lines around their start.  Tags
+// in and enclosing lines out go through shared memory (staged()).
 __global__ void __launch_bounds__(kChunkThreads) resolve_kernel(const uint32_t *tag, const int *depth, const int *meta,
                                                                 int nchunks, const int *sum, const int *blk, int *encl) {
+    __shared__ uint32_t s_tag[kChunk * kStageCols];
+    __shared__ int s_enc[kChunk * kStageCols];
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     const int end = meta[0], L = meta[1];
+    const int b0 = blockIdx.x * kChunkThreads * kChunk;
+    const int cnt = max(0, min(end - b0, kChunkThreads * kChunk));
+    for (int i = threadIdx.x; i < cnt; i += kChunkThreads) s_tag[staged(i)] = tag[b0 + i];
     int st[kMaxDepth + 1];
     st[0] = -1;
     for (int l = 1; l <= L; ++l) {
         const int v = c < nchunks ? sum[(long long)c * kMaxDepth + l - 1] : -1;
         st[l] = max(block_excl_max<kChunkThreads>(v), blk[(long long)blockIdx.x * kMaxDepth + l - 1]);
     }
-    if (c >= nchunks) return;
-    const int b = c * kChunk, e = min(end, b + kChunk);
-    if (b >= e) return;
-    int d = depth[b];
-    for (int k = b; k < e; ++k) {
-        const uint32_t code = code_of(tag[k]);
-        const int dd = min(max(d, 0), kMaxDepth);
-        encl[k] = st[dd];
-        if (code == C_OPEN) {
-            if (d + 1 <= kMaxDepth && d >= 0) st[d + 1] = k;
-            ++d;
-        } else if (code == C_CLOSE) {
-            --d;
+    __syncthreads();
+    if (c < nchunks) {
+        const int b = c * kChunk, e = min(end, b + kChunk);
+        int d = b < e ? depth[b] : 0;
+        for (int k = b; k < e; ++k) {
+            const int i = staged(k - b0);
+            const uint32_t code = code_of(s_tag[i]);
+            const int dd = min(max(d, 0), kMaxDepth);
+            s_enc[i] = st[dd];
+            if (code == C_OPEN) {
+                if (d + 1 <= kMaxDepth && d >= 0) st[d + 1] = k;
+                ++d;
+            } else if (code == C_CLOSE) {
+                --d;
+            }
         }
     }
+    __syncthreads();
+    for (int i = threadIdx.x; i < cnt; i += kChunkThreads) encl[b0 + i] = s_enc[staged(i)];
 }
 
 // ---------------------------------------------------------------------------
@@ -651,6 +759,38 @@ __global__ void lines_kernel(const char *text, LineRange lr, const uint32_t *tag
     }
 }
 
+// A line staged in shared memory: 16-byte loads (single bytes past the
+// text's end) of the aligned chunks covering it, stored as words into this
+// thread's slot of kStageWords (an odd word count, so the 32 slots of a
+// warp start on 32 different banks).  Returns the line's first byte in the
+// slot, or the global pointer when the line does not fit.
+constexpr int kStageWords = 29;  // 116 bytes: lines up to 100 bytes
+__device__ __forceinline__ const char *stage_line(const char *text, long long len, long long s, int n,
+                                                  uint32_t *slot) {
+    const long long a0 = s & ~15LL;
+    if (s + n - a0 > 4 * kStageWords) return text + s;
+    for (long long a = a0; a < s + n; a += 16) {
+        uint32_t *d = slot + (a - a0) / 4;
+        if (a + 16 <= len) {
+            const uint4 v = *reinterpret_cast<const uint4 *>(text + a);
+            d[0] = v.x;
+            d[1] = v.y;
+            d[2] = v.z;
+            d[3] = v.w;
+        } else {
+            for (int w = 0; w < 4; ++w) {
+                uint32_t x = 0;
+                for (int b = 0; b < 4; ++b) {
+                    const long long o = a + 4 * w + b;
+                    if (o < len) x |= (uint32_t)(unsigned char)text[o] << (8 * b);
+                }
+                d[w] = x;
+            }
+        }
+    }
+    return reinterpret_cast<const char *>(slot) + (s - a0);
+}
+
 __device__ bool read_vec(const char *l, int n, double *out) {
     int eq = 0;
     while (eq < n && l[eq] != '=') ++eq;
@@ -666,8 +806,14 @@ __device__ bool read_vec(const char *l, int n, double *out) {
 
 // One thread per (field, node), field-major so that a warp converts one
 // kind of field: 0 mass, 1 position, 2 velocity, 3 index and name.
-__global__ void values_kernel(const char *text, LineRange lr, const uint32_t *tag, int nnodes, Nodes N,
-                              unsigned long long *err) {
+//
+// The m, r and v lines are staged in shared memory first (a few 16-byte
+// loads per line instead of a byte load per character: the 32 lines of a
+// warp lie in 32 different places of the text).
+__global__ void __launch_bounds__(256) values_kernel(const char *text, LineRange lr, const uint32_t *tag, int nnodes,
+                                                     Nodes N, unsigned long long *err) {
+    __shared__ uint32_t stage[256 * kStageWords];
+    uint32_t *slot = stage + threadIdx.x * kStageWords;
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= 4LL * nnodes) return;
     const int f = (int)(t / nnodes), id = (int)(t - (long long)f * nnodes);
@@ -675,17 +821,18 @@ __global__ void values_kernel(const char *text, LineRange lr, const uint32_t *ta
     long long s;
     if (f == 0 && w[FLD_M] >= 0) {
         const int n = lr.span(w[FLD_M], s);
-        const story::Real r = story::parse_real(text + s + voff_of(tag[w[FLD_M]]), text + s + n);
+        const char *l = stage_line(text, lr.len, s, n, slot);
+        const story::Real r = story::parse_real(l + voff_of(tag[w[FLD_M]]), l + n);
         if (r.err) report(err, w[FLD_M] + 1, E_NUMBER);
         N.mass[id] = r.v;
     }
     if (f == 1 && w[FLD_R] >= 0) {
         const int n = lr.span(w[FLD_R], s);
-        if (!read_vec(text + s, n, N.pos + 3 * id)) report(err, w[FLD_R] + 1, E_VECTOR);
+        if (!read_vec(stage_line(text, lr.len, s, n, slot), n, N.pos + 3 * id)) report(err, w[FLD_R] + 1, E_VECTOR);
     }
     if (f == 2 && w[FLD_V] >= 0) {
         const int n = lr.span(w[FLD_V], s);
-        if (!read_vec(text + s, n, N.vel + 3 * id)) report(err, w[FLD_V] + 1, E_VECTOR);
+        if (!read_vec(stage_line(text, lr.len, s, n, slot), n, N.vel + 3 * id)) report(err, w[FLD_V] + 1, E_VECTOR);
     }
     if (f == 3 && w[FLD_I] >= 0) {
         const int n = lr.span(w[FLD_I], s);
@@ -951,6 +1098,9 @@ class Reader {
 
   private:
     std::vector<Buf> bufs_;
+    unsigned long long *d_ticket = nullptr;  // scan tile tickets, counting up across scans
+    unsigned long long ticket_base_ = 0;
+    unsigned scan_epoch_ = 0;
     int *d_meta = nullptr;
     unsigned long long *d_err = nullptr;
     int *h_meta = nullptr;
@@ -1058,6 +1208,7 @@ void Reader::release() {
     bufs_.clear();
     if (d_meta) cudaFree(d_meta);
     if (d_err) cudaFree(d_err);
+    if (d_ticket) cudaFree(d_ticket);
     if (h_meta) cudaFreeHost(h_meta);
     if (h_err) cudaFreeHost(h_err);
     if (stream) cudaStreamDestroy(stream);
@@ -1075,6 +1226,8 @@ int Reader::open() {
     bufs_.resize(S_COUNT);
     if ((e = cudaMalloc(&d_meta, 16 * sizeof(int))) != cudaSuccess) return fail("device memory", e);
     if ((e = cudaMalloc(&d_err, sizeof(unsigned long long))) != cudaSuccess) return fail("device memory", e);
+    if ((e = cudaMalloc(&d_ticket, sizeof(unsigned long long))) != cudaSuccess) return fail("device memory", e);
+    if ((e = cudaMemset(d_ticket, 0, sizeof(unsigned long long))) != cudaSuccess) return fail("device memory", e);
     if ((e = cudaMallocHost(&h_meta, 16 * sizeof(int))) != cudaSuccess) return fail("pinned memory", e);
     if ((e = cudaMallocHost(&h_err, sizeof(unsigned long long))) != cudaSuccess) return fail("pinned memory", e);
     if ((e = cudaFuncSetAttribute(correct_big_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kBigSmem)) !=
@@ -1086,11 +1239,17 @@ int Reader::open() {
 template <class F>
 int Reader::scan(F f, long long n, int *out, int *total, int slot) {
     const int tiles = (int)std::max<long long>(1, (n + kScanTile - 1) / kScanTile);
-    int *ts;
-    if (ensure(slot, ts, (size_t)tiles)) return -1;
-    tile_sum_kernel<<<tiles, 256, 0, stream>>>(f, n, ts);
-    scan_tiles_kernel<<<1, 1024, 0, stream>>>(ts, tiles, total);
-    tile_apply_kernel<<<tiles, 256, 0, stream>>>(f, n, ts, out);
+    unsigned long long *st;
+    const size_t cap_before = bufs_[slot].cap;
+    if (ensure(slot, st, (size_t)tiles)) return -1;
+    if (bufs_[slot].cap != cap_before) cudaMemsetAsync(st, 0, bufs_[slot].cap, stream);  // epoch 0: never current
+    ++scan_epoch_;
+    if (scan_epoch_ >= (1u << 30)) {  // the epoch field wrapped: start over on zeroed words
+        scan_epoch_ = 1;
+        cudaMemsetAsync(st, 0, bufs_[slot].cap, stream);
+    }
+    scan1_kernel<<<tiles, 256, 0, stream>>>(f, n, out, total, st, d_ticket, ticket_base_, scan_epoch_, tiles, d_err);
+    ticket_base_ += (unsigned long long)tiles;
     return 0;
 }
 
@@ -1133,6 +1292,8 @@ int Reader::parse(const char *text, long long len, bool on_device, int flags, g6
         d_text = t;
     }
     cudaMemsetAsync(d_err, 0xff, sizeof(unsigned long long), stream);
+    cudaMemsetAsync(d_ticket, 0, sizeof(unsigned long long), stream);
+    ticket_base_ = 0;
     const int init_meta[16] = {0x7fffffff, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
     memcpy(h_meta, init_meta, sizeof init_meta);
     cudaMemcpyAsync(d_meta, h_meta, sizeof init_meta, cudaMemcpyHostToDevice, stream);

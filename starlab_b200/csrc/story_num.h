@@ -20,10 +20,19 @@
 //      (registers) cover |q| <= 27 with up to 19 digits (every number the
 //      reference writes at its default 18 digits); larger exponents or more
 //      digits use 20 words.
+// Before step 2, up to 19 digits (w < 2^64) go through the Eisel-Lemire
+// conversion: w normalised times a 128-bit approximation of 5^q
+// (pow5_table.h), whose leading bits are the rounded significand -- exact
+// for every w < 2^64 and every q of the table (Lemire 2021, "Number parsing
+// at a gigabyte per second"; Mushtak and Lemire 2023, "Fast number parsing
+// without fallback"), with the exact ties-to-even test for the q where a
+// decimal can lie halfway between two doubles (-4 <= q <= 23).  Step 2
+// then only sees more than 19 digits.
 // Forms the reference never writes -- hexadecimal floats, NaN payloads
 // "nan(...)", more than 40 significant digits -- are reported, not guessed.
 #pragma once
 #include <stdint.h>
+#include "pow5_table.h"
 
 #if defined(__CUDACC__)
 #define SN_HD __host__ __device__ __forceinline__
@@ -136,6 +145,65 @@ SN_HD double pow10_exact(int k) {  // 10^k for 0 <= k <= 22, exact
     if (k & 8) r *= 1e8;
     if (k & 16) r *= 1e16;
     return r;
+}
+
+#if defined(__CUDACC__)
+__device__ static const uint64_t kPow5Dev[] = SN_POW5_TABLE;
+#endif
+static const uint64_t kPow5Host[] = SN_POW5_TABLE;
+
+SN_HD uint64_t pow5_word(int k) {
+#if defined(__CUDA_ARCH__)
+    return __ldg(&kPow5Dev[k]);
+#else
+    return kPow5Host[k];
+#endif
+}
+
+SN_HD int clz64(uint64_t x) {
+#if defined(__CUDA_ARCH__)
+    return __clzll((long long)x);
+#else
+    return __builtin_clzll(x);
+#endif
+}
+
+// Eisel-Lemire: the bits of the double nearest w * 10^q (w < 2^64, w > 0,
+// SN_POW5_MIN_Q <= q <= SN_POW5_MAX_Q), sign not included.
+SN_HD uint64_t eisel_lemire(uint64_t w, int q) {
+    const int lz = clz64(w);
+    w <<= lz;
+    const int idx = 2 * (q - SN_POW5_MIN_Q);
+    // 128-bit product of w with the table's high word; the low word only
+    // when the product's bits below the 55 kept ones are all ones
+    uint64_t lo = w * pow5_word(idx), hi = mul_hi64(w, pow5_word(idx));
+    if ((hi & 0x1ffu) == 0x1ffu) {
+        const uint64_t lo2 = mul_hi64(w, pow5_word(idx + 1));
+        lo += lo2;
+        hi += lo < lo2;
+    }
+    const int upper = (int)(hi >> 63);
+    const int shift = upper + 9;
+    uint64_t m = hi >> shift;
+    // binary exponent: floor(q log2 10) + 63, + the product's top bit, - lz, + the bias 1023
+    int p2 = (((152170 + 65536) * q) >> 16) + 63 + upper - lz + 1023;
+    if (p2 <= 0) {  // subnormal
+        if (-p2 + 1 >= 64) return 0;
+        m >>= -p2 + 1;
+        m += m & 1;
+        m >>= 1;
+        return m;  // 2^52 when it rounded up to the smallest normal: the same bits
+    }
+    if (lo <= 1 && q >= -4 && q <= 23 && (m & 3) == 1 && (m << shift) == hi) m &= ~(uint64_t)1;  // exact tie: to even
+    m += m & 1;
+    m >>= 1;
+    if (m >= (2ull << 52)) {
+        m = 1ull << 52;
+        ++p2;
+    }
+    m &= ~(1ull << 52);
+    if (p2 >= 0x7ff) return 0x7ff0000000000000ull;
+    return m | ((uint64_t)p2 << 52);
 }
 
 SN_HD bool is_space(char c) { return c == ' ' || (c >= '\t' && c <= '\r'); }
@@ -456,6 +524,12 @@ SN_HD Real parse_real(const char *p, const char *e) {
         const double wd = (double)w0;
         r.v = qi >= 0 ? wd * pow10_exact(qi) : wd / pow10_exact(-qi);
         if (neg) r.v = -r.v;
+        return r;
+    }
+    if (!big) {
+        // q + nd in [-324, 309] with nd <= 19: q <= 308; below the table
+        // (q = -343) w * 10^q < 10^-324, under half the smallest subnormal
+        r.v = from_bits((qi < SN_POW5_MIN_Q ? 0 : eisel_lemire(w0, qi)) | sign);
         return r;
     }
     // Candidate: w as a double, scaled by powers of ten in steps of at most

@@ -141,6 +141,37 @@ def test_halfway_cases_round_to_even(shim):
     check(shim, strs)
 
 
+def test_up_to_19_digits_near_midpoints(shim):
+    """The Eisel-Lemire path (at most 19 significant digits): the closest
+    17-, 18- and 19-digit decimals on both sides of the midpoint between a
+    double and its upper neighbour, over normal and subnormal doubles and
+    every binary exponent, plus exact ties that fit in 19 digits."""
+    from decimal import ROUND_CEILING, ROUND_FLOOR
+    getcontext().prec = 800
+    rng = np.random.default_rng(6)
+    xs = [x for x in rand_doubles(rng, 6000) if x > 0]
+    xs += list((rng.integers(1, 2**52, size=1000, dtype=np.uint64)).view(np.float64))
+    strs = []
+    for x in xs:
+        nx = float(np.nextafter(x, np.inf))
+        if not np.isfinite(nx):
+            continue
+        mid = (Decimal(float(x)) + Decimal(nx)) / 2
+        for nd in (17, 18, 19):
+            q = Decimal(1).scaleb(mid.adjusted() - nd + 1)
+            for rnd in (ROUND_FLOOR, ROUND_CEILING):
+                strs.append("%se%d" % (mid.quantize(q, rounding=rnd).scaleb(-q.adjusted()).to_integral_value(),
+                                       q.adjusted()))
+    for e in range(53, 63):  # integer ties: 2^e + odd * 2^(e - 53)
+        for k in rng.integers(0, 2**51, size=40):
+            strs.append(str(2**e + (2 * int(k) + 1) * 2 ** (e - 53)))
+    for e in range(48, 53):  # ties with a short binary fraction
+        for k in rng.integers(0, 2**51, size=40):
+            t = Decimal(2**e) + Decimal(2 * int(k) + 1) * Decimal(2) ** (e - 53)
+            strs.append(format(t, "f"))
+    check(shim, strs)
+
+
 def test_subnormals_overflow_and_zero(shim):
     rng = np.random.default_rng(4)
     sub = (rng.integers(1, 2**52, size=3000, dtype=np.uint64)).view(np.float64)
