@@ -249,7 +249,8 @@ struct StateMixedP {
     float2 nxh, nyh, nzh, nxl, nyl, nzl, nvx, nvy, nvz;
     float h2;
     float2 ax, ay, az, jx, jy, jz, pm;  // FP32 sums since the last fold; pm = sum m/(4r)
-    unsigned qa0, qa1, qj0, qj1;        // error indicators (kVarStats): bits of max m/(2r^2), max m/r^3
+    unsigned qa0, qa1;                  // error indicators (kVarStats): bits of max m/(2r^2) (unsigned max)
+    int qj0, qj1;                       // and of max m/r^3 (signed max: the self term's -0.0 never wins)
     double Ax, Ay, Az, Jx, Jy, Jz, Pt;
     float nr2;
     int nj, idx, i;
@@ -275,7 +276,8 @@ __device__ __forceinline__ void load_i(StateMixedP &s, const IRec &q, const Forc
     s.h2 = (float)q.h2;
     s.idx = q.index;
     s.ax = s.ay = s.az = s.jx = s.jy = s.jz = s.pm = make_float2(0.f, 0.f);
-    s.qa0 = s.qa1 = s.qj0 = s.qj1 = 0u;
+    s.qa0 = s.qa1 = 0u;
+    s.qj0 = s.qj1 = 0;
     s.Ax = s.Ay = s.Az = s.Jx = s.Jy = s.Jz = s.Pt = 0.0;
     s.nr2 = FLT_MAX;
     s.nj = -1;
@@ -350,15 +352,18 @@ __device__ __forceinline__ void interact_pair(StateMixedP &s, const JPairMixed &
     const float2 a3 = __fmul2_rn(__fmul2_rn(rv, dup(-0.75f)), r2inv);
     if (STATS) {
         // The refinement's error indicators, the largest single terms:
-        // mr y = -m/(2 r^2) (y is -2/r, see above) and mr3 = m/r^3 (self:
-        // m = 0).  Non-positive (resp. non-negative) floats order like their
-        // bit patterns read as unsigned, so the maxima are integer maxima,
-        // off the FMA pipe.
+        // mr y = -m/(2 r^2) (y is -2/r, see above) and mr3 = m/r^3.  The
+        // maxima are integer maxima of the bit patterns, off the FMA pipe:
+        // non-positive floats order like their bits read as unsigned (t),
+        // non-negative ones like their bits read as signed (mr3).  The self
+        // term (m = +0, y < 0) gives mr3 = -0.0, whose bits 0x80000000 would
+        // win an unsigned maximum over every positive float; as a signed
+        // int it is the smallest value.
         const float2 t = __fmul2_rn(mr, y);
         s.qa0 = max(s.qa0, __float_as_uint(t.x));
         s.qa1 = max(s.qa1, __float_as_uint(t.y));
-        s.qj0 = max(s.qj0, __float_as_uint(mr3.x));
-        s.qj1 = max(s.qj1, __float_as_uint(mr3.y));
+        s.qj0 = max(s.qj0, __float_as_int(mr3.x));
+        s.qj1 = max(s.qj1, __float_as_int(mr3.y));
     }
     s.pm = __fadd2_rn(s.pm, mr);
     s.ax = __ffma2_rn(mr3, dx, s.ax);
@@ -540,7 +545,7 @@ __device__ __forceinline__ void to_partial(const StateMixedP &s, Partial &q) {
     q.nn_r2 = (double)s.nr2;
     q.nn_j = s.nj;
     q.qa = -2.f * __uint_as_float(max(s.qa0, s.qa1));  // max m / r^2
-    q.qj = __uint_as_float(max(s.qj0, s.qj1));         // max m / r^3
+    q.qj = __int_as_float(max(s.qj0, s.qj1));          // max m / r^3
 }
 __device__ __forceinline__ void to_partial(const StateF64 &s, Partial &q) {
     q.acc[0] = s.Ax; q.acc[1] = s.Ay; q.acc[2] = s.Az;

@@ -268,7 +268,7 @@ def test_deterministic_repeat(c2):
     eng.close()
 
 
-def _all_i_errors(n, seed, eps2, ti, masses=None):
+def _all_i_errors(n, seed, eps2, ti, masses=None, cfg=None):
     """Every particle of an n-body snapshot at a predicted block time, mixed
     mode against the engine's FP64 mode (itself within 1e-12 of the oracle:
     checked on a sample here too).  acc and jerk for the predictor from one
@@ -284,6 +284,8 @@ def _all_i_errors(n, seed, eps2, ti, masses=None):
     e64.set_ti(ti)
     ref = e64.sweep(n, eps2=eps2)
     emx = new_engine("mixed", npipes=n)
+    if cfg is not None:
+        emx.set_config(*cfg)
     emx.set_j_particles(0.0, m, jerk / 6.0, 0.5 * acc, v, x)
     emx.set_ti(ti)
     got = emx.sweep(n, eps2=eps2)
@@ -291,6 +293,25 @@ def _all_i_errors(n, seed, eps2, ti, masses=None):
     e64.close()
     emx.close()
     return (m, x, v, acc, jerk), got, ref, refined
+
+
+@pytest.mark.parametrize("nsplit", [1, 2, 3])
+def test_refinement_does_not_depend_on_the_split(nsplit):
+    """The refinement's indicators are maxima over all j, whatever the
+    j-split: every particle of the N = 262144 sweep within the contract
+    with the j-range in one, two and three splits.  (With an unsigned
+    maximum over the bit patterns the self term's -0.0 won, and the jerk
+    indicator of every split holding the particle itself was lost: one
+    split meant no jerk flag at all.)"""
+    from starlab_b200 import ics
+    n = 262144
+    state, got, ref, refined = _all_i_errors(n, 11, 1e-8, 13.0 / 1024, masses=ics.salpeter_masses(n, 12),
+                                             cfg=(32, 1, 8, 1, nsplit))
+    ea, ej, ep = rel_err_vec(got[0], ref[0]), rel_err_vec(got[1], ref[1]), rel_err(got[2], ref[2])
+    print("nsplit %d: acc max %.2e jerk max %.2e pot max %.2e refined %d" % (nsplit, ea.max(), ej.max(), ep.max(),
+                                                                           refined))
+    assert ea.max() <= 1e-6 and ej.max() <= 1e-5 and ep.max() <= 1e-6, (float(ea.max()), float(ej.max()))
+    assert 0.01 * n < refined < 0.05 * n
 
 
 @pytest.mark.parametrize("case", ["c2", "c3"])
