@@ -91,6 +91,7 @@ Engine::Engine(int cluster_id) : cluster_id_(cluster_id) {
     event_timing_ = getenv("G6B200_EVENT_TIMING") != nullptr;
     fault_pot_at_ = env_ll("G6B200_FAULT_POT", -1);
     small_enabled_ = env_int("G6B200_SMALL_CALLS", 1) != 0;
+    refine_enabled_ = env_int("G6B200_REFINE", 1) != 0;
 }
 
 Engine::~Engine() { close(); }
@@ -131,6 +132,7 @@ int Engine::open(int device, int nmax_hint) {
     *h_ref_count_ = 0;
     G6_CHECK(cudaMalloc(&d_v2_, sizeof(double) * (kRefineBlocks + 1)), "refine");
     G6_CHECK(cudaMalloc(&d_ref_small_, sizeof(int) * 8), "refine");
+    G6_CHECK(cudaMemset(d_ref_small_, 0, sizeof(int) * 8), "refine");  // flag count and block counter start at 0
     G6_CHECK(cudaMalloc(&d_ref_items_, sizeof(ForceParams)), "refine");
     open_ = true;
     if (ensure_capacity(std::max(nmax_hint, 1024) - 1)) return -1;
@@ -159,10 +161,10 @@ void Engine::close() {
     hfree(h_irec_); hfree(h_out_); hfree(h_nb_off_); hfree(h_nb_count_); hfree(h_bulk_);
     hfree(h_ieps2_); dfree(d_ieps2_); hfree(h_energy_); dfree(d_energy_);
     hfree(h_ref_count_); dfree(d_v2_); dfree(d_ref_small_); dfree(d_ref_items_); dfree(d_q_);
-    dfree(d_ref_list_); dfree(d_ref_tcnt_); dfree(d_ref_nn_); dfree(d_ref_irec_); dfree(d_ref_out_);
+    dfree(d_ref_list_); dfree(d_ref_tcnt_); dfree(d_ref_irec_);
     dfree(d_ref_part_); dfree(d_jrec64_);
     h_ref_count_ = nullptr; d_v2_ = nullptr; d_ref_small_ = nullptr; d_ref_items_ = nullptr; d_q_ = nullptr;
-    d_ref_list_ = nullptr; d_ref_tcnt_ = nullptr; d_ref_nn_ = nullptr; d_ref_irec_ = nullptr; d_ref_out_ = nullptr;
+    d_ref_list_ = nullptr; d_ref_tcnt_ = nullptr; d_ref_irec_ = nullptr;
     d_ref_part_ = nullptr; d_jrec64_ = nullptr; ref_cap_ = 0; jrec64_cap_ = 0;
     pred64_valid_ = v2_valid_ = false;
     cudaEvent_t evs[] = {ev_stage_, ev_begin_, ev_pred0_, ev_pred1_, ev_force0_, ev_force1_, ev_done_};
@@ -517,18 +519,14 @@ int Engine::ensure_refine_buffers(int ni) {
     if (ni > ref_cap_) {
         const int n = std::max(ni, npipes_);
         auto dfree = [](void *p) { if (p) cudaFree(p); };
-        dfree(d_q_); dfree(d_ref_list_); dfree(d_ref_tcnt_); dfree(d_ref_nn_); dfree(d_ref_irec_);
-        dfree(d_ref_out_); dfree(d_ref_part_);
-        d_q_ = nullptr; d_ref_list_ = d_ref_tcnt_ = d_ref_nn_ = nullptr; d_ref_irec_ = nullptr;
-        d_ref_out_ = nullptr; d_ref_part_ = nullptr;
+        dfree(d_q_); dfree(d_ref_list_); dfree(d_ref_tcnt_); dfree(d_ref_irec_); dfree(d_ref_part_);
+        d_q_ = nullptr; d_ref_list_ = d_ref_tcnt_ = nullptr; d_ref_irec_ = nullptr; d_ref_part_ = nullptr;
         ref_cap_ = 0;
         G6_CHECK(cudaMalloc(&d_q_, sizeof(float) * 2 * (size_t)n), "refine");
         G6_CHECK(cudaMalloc(&d_ref_list_, sizeof(int) * (size_t)n), "refine");
         G6_CHECK(cudaMalloc(&d_ref_tcnt_, sizeof(int) * (size_t)n), "refine");
         G6_CHECK(cudaMemsetAsync(d_ref_tcnt_, 0, sizeof(int) * (size_t)n, stream_), "refine");
-        G6_CHECK(cudaMalloc(&d_ref_nn_, sizeof(int) * (size_t)n), "refine");
         G6_CHECK(cudaMalloc(&d_ref_irec_, sizeof(IRec) * (size_t)n), "refine");
-        G6_CHECK(cudaMalloc(&d_ref_out_, sizeof(double) * 7 * (size_t)n), "refine");
         G6_CHECK(cudaMalloc(&d_ref_part_, sizeof(Partial) * refine_partial_records(n)), "refine");
         ref_cap_ = n;
         stats_.grows++;
@@ -760,7 +758,7 @@ int Engine::launch_call() {
         // Mixed mode (paired layout): ill-conditioned particles are
         // recomputed in FP64 (refine.cu); not for potential-only, j-split
         // or GRAPE-4 calls.
-        call_refine_ = km == kKernMixedP && !pot_k && !call_split_ && !call_g4_;
+        call_refine_ = refine_enabled_ && km == kKernMixedP && !pot_k && !call_split_ && !call_g4_;
         if (call_refine_ && ensure_refine_buffers(ni)) return -1;
         if (call_split_) cfg.jper = call_split_;
         if (ensure_call_buffers(ni, call_nb_, call_split_ ? partial_bytes_fixed(call_split_, nj_pad, ni)
@@ -825,19 +823,16 @@ int Engine::launch_call() {
             ra.count = d_ref_small_;
             ra.counter = d_ref_small_ + 1;
             ra.pre = d_ref_small_ + 2;
+            ra.done = reinterpret_cast<unsigned *>(d_ref_small_ + 6);
             ra.list = d_ref_list_;
             ra.irec_ref = d_ref_irec_;
-            ra.racc = d_ref_out_;
-            ra.rjerk = d_ref_out_ + 3 * (size_t)ref_cap_;
-            ra.rpot = d_ref_out_ + 6 * (size_t)ref_cap_;
-            ra.rnn = d_ref_nn_;
             ra.part = d_ref_part_;
             ra.tcnt = d_ref_tcnt_;
             ra.items = d_ref_items_;
             ra.status = status;
             G6_CHECK(launch_refine(stream_, ra, num_sms_), "refine launch");
-            stats_.launches += 5;
-            G6_CHECK(cudaMemcpyAsync(h_ref_count_, d_ref_small_, sizeof(int), cudaMemcpyDeviceToHost, stream_),
+            stats_.launches += 2;
+            G6_CHECK(cudaMemcpyAsync(h_ref_count_, d_ref_small_ + 5, sizeof(int), cudaMemcpyDeviceToHost, stream_),
                      "refine count");
         }
         if (call_split_) {

@@ -224,6 +224,7 @@ class Engine {
     // Small calls (<= kSmallMax i and staged j-updates): one launch carries
     // the host data as its parameter (G6B200_SMALL_CALLS=0 turns it off).
     bool small_enabled_ = true;
+    bool refine_enabled_ = true;  // G6B200_REFINE=0: mixed mode without the FP64 recomputation
     bool call_small_ = false;
     int small_parity_ = 0;  // status word the next small call reports into
     int call_parity_ = 0;   // status word of the call in flight
@@ -243,12 +244,11 @@ class Engine {
     int ensure_refine_buffers(int ni);
     int ref_cap_ = 0;
     float *d_q_ = nullptr;            // [ref_cap_][2] error indicators
-    int *d_ref_list_ = nullptr, *d_ref_tcnt_ = nullptr, *d_ref_nn_ = nullptr;
+    int *d_ref_list_ = nullptr, *d_ref_tcnt_ = nullptr;
     IRec *d_ref_irec_ = nullptr;
-    double *d_ref_out_ = nullptr;     // acc [3 cap], jerk [3 cap], pot [cap]
     Partial *d_ref_part_ = nullptr;
     ForceParams *d_ref_items_ = nullptr;
-    int *d_ref_small_ = nullptr;      // count, counter, pre[4]
+    int *d_ref_small_ = nullptr;      // count, counter, pre[4] (pre[3]: the last call's flag count), done
     double *d_v2_ = nullptr;          // [kRefineBlocks + 1]
     void *d_jrec64_ = nullptr;        // FP64 records of the refinement [cap_]
     int jrec64_cap_ = 0;

@@ -605,16 +605,17 @@ __device__ __forceinline__ Partial load_partial_cg(const Partial *src) {
 }
 
 __device__ __forceinline__ void write_final(const ForceParams &p, int i, const Partial &q) {
+    const size_t o = p.out_map ? (size_t)p.out_map[i] : (size_t)i;
 #pragma unroll
     for (int c = 0; c < 3; c++) {
-        p.out_acc[3 * i + c] = q.acc[c];
-        p.out_jerk[3 * i + c] = q.jerk[c];
+        p.out_acc[3 * o + c] = q.acc[c];
+        p.out_jerk[3 * o + c] = q.jerk[c];
     }
-    p.out_pot[i] = q.pot;
-    p.out_nn[i] = (q.nn_j < 0 || q.nn_j >= p.nj) ? 0 : q.nn_j;
+    p.out_pot[o] = q.pot;
+    p.out_nn[o] = (q.nn_j < 0 || q.nn_j >= p.nj) ? 0 : q.nn_j;
     if (p.out_q) {
-        p.out_q[2 * (size_t)i] = q.qa;
-        p.out_q[2 * (size_t)i + 1] = q.qj;
+        p.out_q[2 * o] = q.qa;
+        p.out_q[2 * o + 1] = q.qj;
     }
 }
 

@@ -72,6 +72,10 @@ struct ForceParams {
     // Mixed-mode error indicators (qa, qj of Partial) per i, [ni][2], when
     // the kernel accumulates them (single-call paired mixed kernels).
     float *out_q;
+    // When set: the results of i go to row out_map[i] of the outputs (the
+    // refinement's FP64 pass writes its particles' rows of the call's
+    // outputs directly).
+    const int *out_map;
 };
 
 // A batch of calls for the persistent multi-item kernel (device pointers).
@@ -265,15 +269,14 @@ struct RefineArgs {
     const void *jrec64;       // JRecF64 [nj_pad] at the call's block time
     double *acc, *jerk, *pot; // the call's outputs, refined in place
     int *nn;
-    int *count, *list;        // flagged count, [ni] flagged i
+    int *count, *list;        // flagged count (zero between calls), [ni] flagged i
     IRec *irec_ref;           // [ni]
-    double *racc, *rjerk, *rpot;  // [ni] FP64 pass outputs
-    int *rnn;
     Partial *part;            // refine_partial_records(ni)
     int *tcnt;                // [ni] i-tile counters, zero between calls
     ForceParams *items;       // [1]
-    int *pre;                 // [4]
+    int *pre;                 // [4]: task and i prefix sums of the FP64 item; pre[3] = flagged count
     int *counter;
+    unsigned *done;           // flag blocks finished, zero between calls
     unsigned *status;
 };
 void launch_refine_v2(cudaStream_t s, const double *jraw, int cap, int nj, double *work);

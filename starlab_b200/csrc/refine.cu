@@ -60,54 +60,66 @@ __global__ void __launch_bounds__(kThreads) v2_total_kernel(double *work, int nj
     if (threadIdx.x == 0) work[kRefineBlocks] = nj > 0 ? s / nj : 0.0;  // mean |v|^2
 }
 
-__global__ void flag_kernel(int ni, const double *__restrict__ acc, const double *__restrict__ jerk,
-                            const float *__restrict__ q, const double *__restrict__ v2, int *__restrict__ count,
-                            int *__restrict__ list, const IRec *__restrict__ irec, IRec *__restrict__ irec_ref) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= ni) return;
-    const double vrms = sqrt(v2[kRefineBlocks]);
-    const double a2 = acc[3 * (size_t)i] * acc[3 * (size_t)i] + acc[3 * (size_t)i + 1] * acc[3 * (size_t)i + 1] +
-                      acc[3 * (size_t)i + 2] * acc[3 * (size_t)i + 2];
-    const double j2 = jerk[3 * (size_t)i] * jerk[3 * (size_t)i] + jerk[3 * (size_t)i + 1] * jerk[3 * (size_t)i + 1] +
-                      jerk[3 * (size_t)i + 2] * jerk[3 * (size_t)i + 2];
-    const double qa = q[2 * (size_t)i], qj = q[2 * (size_t)i + 1];
-    // flagged unless both ratios are finite and within their bounds
-    const bool good = qa * qa <= kRefineA * kRefineA * a2 && qj * qj * vrms * vrms <= kRefineJ * kRefineJ * j2;
-    if (good) return;
-    const int k = atomicAdd(count, 1);
-    list[k] = i;
-    irec_ref[k] = irec[i];
-}
-
-// One thread: the FP64 pass's single work item, sized by the flag count.
-__global__ void setup_kernel(ForceParams base, ForceConfig cfg, const int *__restrict__ count,
-                             ForceParams *__restrict__ items, int *__restrict__ pre, int *__restrict__ counter) {
-    ForceParams p = base;
-    p.ni = *count;
+// One FP64 work item for the flagged particles, sized by their count.
+// Tasks wanted: one per kMinTaskWork interactions (as the servers' plan),
+// but no fewer than kRefineMinTasks -- a call with a handful of flagged
+// particles otherwise ran as a dozen CTAs walking long j-ranges (ni = 128:
+// 0.32 ms with the refinement vs 0.12 ms without) -- and no more than 592.
+// The item writes its results straight into the flagged particles' rows of
+// the call's outputs (out_map = the flag list).
+constexpr int kRefineMinTasks = 128;
+__device__ void make_refine_item(ForceParams p, ForceConfig cfg, int count, ForceParams *items, int *pre,
+                                 int *counter) {
+    p.ni = count;
+    const long long wc = (long long)p.ni * p.nj_pad / kMinTaskWork;
+    cfg.nsplit = (int)(wc < kRefineMinTasks ? kRefineMinTasks : (wc > 592 ? 592 : wc));
     int nt = 0;
     batch_plan(kKernF64, cfg, p, nt);
     items[0] = p;
-    pre[0] = 0;       // task0
+    pre[0] = 0;  // task0
     pre[1] = nt;
-    pre[2] = 0;       // ipre
+    pre[2] = 0;  // ipre
     pre[3] = p.ni;
     *counter = 0;
 }
 
-__global__ void scatter_kernel(int ni_max, const int *__restrict__ count, const int *__restrict__ list,
-                               const double *__restrict__ racc, const double *__restrict__ rjerk,
-                               const double *__restrict__ rpot, const int *__restrict__ rnn, double *__restrict__ acc,
-                               double *__restrict__ jerk, double *__restrict__ pot, int *__restrict__ nn) {
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= ni_max || k >= *count) return;
-    const int i = list[k];
-#pragma unroll
-    for (int c = 0; c < 3; ++c) {
-        acc[3 * (size_t)i + c] = racc[3 * (size_t)k + c];
-        jerk[3 * (size_t)i + c] = rjerk[3 * (size_t)k + c];
+// Flag and compact the ill-conditioned particles; the last block to finish
+// builds the FP64 pass's work item, then zeroes the flag count and its own
+// arrival counter for the next call (the count stays readable in pre[3]).
+__global__ void flag_kernel(int ni, const double *__restrict__ acc, const double *__restrict__ jerk,
+                            const float *__restrict__ q, const double *__restrict__ v2, int *__restrict__ count,
+                            int *__restrict__ list, const IRec *__restrict__ irec, IRec *__restrict__ irec_ref,
+                            ForceParams base, ForceConfig cfg, ForceParams *__restrict__ items, int *__restrict__ pre,
+                            int *__restrict__ counter, unsigned *__restrict__ done) {
+    __shared__ bool s_last;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < ni) {
+        const double vrms = sqrt(v2[kRefineBlocks]);
+        const double a2 = acc[3 * (size_t)i] * acc[3 * (size_t)i] + acc[3 * (size_t)i + 1] * acc[3 * (size_t)i + 1] +
+                          acc[3 * (size_t)i + 2] * acc[3 * (size_t)i + 2];
+        const double j2 = jerk[3 * (size_t)i] * jerk[3 * (size_t)i] +
+                          jerk[3 * (size_t)i + 1] * jerk[3 * (size_t)i + 1] +
+                          jerk[3 * (size_t)i + 2] * jerk[3 * (size_t)i + 2];
+        const double qa = q[2 * (size_t)i], qj = q[2 * (size_t)i + 1];
+        // flagged unless both ratios are finite and within their bounds
+        const bool good = qa * qa <= kRefineA * kRefineA * a2 && qj * qj * vrms * vrms <= kRefineJ * kRefineJ * j2;
+        if (!good) {
+            const int k = atomicAdd(count, 1);
+            list[k] = i;
+            irec_ref[k] = irec[i];
+        }
     }
-    pot[i] = rpot[k];
-    nn[i] = rnn[k];
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        s_last = atomicAdd(done, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!s_last || threadIdx.x != 0) return;
+    __threadfence();
+    make_refine_item(base, cfg, atomicAdd(count, 0), items, pre, counter);
+    *count = 0;
+    *done = 0;
 }
 
 }  // namespace
@@ -120,9 +132,6 @@ void launch_refine_v2(cudaStream_t s, const double *jraw, int cap, int nj, doubl
 cudaError_t launch_refine(cudaStream_t s, const RefineArgs &r, int num_sms) {
     const int ni = r.ni;
     if (ni <= 0) return cudaSuccess;
-    cudaError_t e = cudaMemsetAsync(r.count, 0, sizeof(int), s);
-    if (e != cudaSuccess) return e;
-    flag_kernel<<<(ni + 255) / 256, 256, 0, s>>>(ni, r.acc, r.jerk, r.q, r.v2, r.count, r.list, r.irec, r.irec_ref);
     ForceConfig cfg = batch_config(kKernF64);
     ForceParams base{};
     base.jrec = r.jrec64;
@@ -131,13 +140,15 @@ cudaError_t launch_refine(cudaStream_t s, const RefineArgs &r, int num_sms) {
     base.irec = r.irec_ref;
     base.eps2 = r.eps2;
     base.part = r.part;
-    base.out_acc = r.racc;
-    base.out_jerk = r.rjerk;
-    base.out_pot = r.rpot;
-    base.out_nn = r.rnn;
+    base.out_acc = r.acc;  // rows list[k] of the call's outputs
+    base.out_jerk = r.jerk;
+    base.out_pot = r.pot;
+    base.out_nn = r.nn;
+    base.out_map = r.list;
     base.status = r.status;
     base.tile_counter = r.tcnt;  // the last CTA of an i-tile adds its splits
-    setup_kernel<<<1, 1, 0, s>>>(base, cfg, r.count, r.items, r.pre, r.counter);
+    flag_kernel<<<(ni + 255) / 256, 256, 0, s>>>(ni, r.acc, r.jerk, r.q, r.v2, r.count, r.list, r.irec, r.irec_ref,
+                                                 base, cfg, r.items, r.pre, r.counter, r.done);
     BatchArgs a;
     a.items = r.items;
     a.task0 = r.pre;
@@ -146,10 +157,8 @@ cudaError_t launch_refine(cudaStream_t s, const RefineArgs &r, int num_sms) {
     a.H = cfg.H;
     a.counter = r.counter;
     a.one_task_per_cta = 0;
-    e = launch_force_batch(s, kKernF64, cfg, a, batch_ctas(kKernF64, cfg, num_sms), 0, false, r.ident);
+    cudaError_t e = launch_force_batch(s, kKernF64, cfg, a, batch_ctas(kKernF64, cfg, num_sms), 0, false, r.ident);
     if (e != cudaSuccess) return e;
-    scatter_kernel<<<(ni + 255) / 256, 256, 0, s>>>(ni, r.count, r.list, r.racc, r.rjerk, r.rpot, r.rnn, r.acc,
-                                                    r.jerk, r.pot, r.nn);
     return cudaGetLastError();
 }
 
