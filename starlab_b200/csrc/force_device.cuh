@@ -249,8 +249,8 @@ struct StateMixedP {
     float2 nxh, nyh, nzh, nxl, nyl, nzl, nvx, nvy, nvz;
     float h2;
     float2 ax, ay, az, jx, jy, jz, pm;  // FP32 sums since the last fold; pm = sum m/(4r)
-    unsigned qa0, qa1;                  // error indicators (kVarStats): bits of max m/(2r^2) (unsigned max)
-    int qj0, qj1;                       // and of max m/r^3 (signed max: the self term's -0.0 never wins)
+    unsigned qa;                        // error indicators (kVarStats): bits of max m/(2r^2) (unsigned max)
+    int qj;                             // and of max m/r^3 (signed max: the self term's -0.0 never wins)
     double Ax, Ay, Az, Jx, Jy, Jz, Pt;
     float nr2;
     int nj, idx, i;
@@ -276,8 +276,8 @@ __device__ __forceinline__ void load_i(StateMixedP &s, const IRec &q, const Forc
     s.h2 = (float)q.h2;
     s.idx = q.index;
     s.ax = s.ay = s.az = s.jx = s.jy = s.jz = s.pm = make_float2(0.f, 0.f);
-    s.qa0 = s.qa1 = 0u;
-    s.qj0 = s.qj1 = 0;
+    s.qa = 0u;
+    s.qj = 0;
     s.Ax = s.Ay = s.Az = s.Jx = s.Jy = s.Jz = s.Pt = 0.0;
     s.nr2 = FLT_MAX;
     s.nj = -1;
@@ -359,11 +359,11 @@ __device__ __forceinline__ void interact_pair(StateMixedP &s, const JPairMixed &
         // term (m = +0, y < 0) gives mr3 = -0.0, whose bits 0x80000000 would
         // win an unsigned maximum over every positive float; as a signed
         // int it is the smallest value.
+        // Both halves of the pair go into one register per indicator with a
+        // three-input maximum.
         const float2 t = __fmul2_rn(mr, y);
-        s.qa0 = max(s.qa0, __float_as_uint(t.x));
-        s.qa1 = max(s.qa1, __float_as_uint(t.y));
-        s.qj0 = max(s.qj0, __float_as_int(mr3.x));
-        s.qj1 = max(s.qj1, __float_as_int(mr3.y));
+        s.qa = __vimax3_u32(s.qa, __float_as_uint(t.x), __float_as_uint(t.y));
+        s.qj = __vimax3_s32(s.qj, __float_as_int(mr3.x), __float_as_int(mr3.y));
     }
     s.pm = __fadd2_rn(s.pm, mr);
     s.ax = __ffma2_rn(mr3, dx, s.ax);
@@ -432,8 +432,8 @@ constexpr int kVarG4 = 4;
 // 8 = potential only (paired mixed and FP64 layouts): the energy sweeps.
 constexpr int kVarPot = 8;
 // 16 = paired mixed layout: also track the refinement's error indicators
-// (the largest single acc and jerk terms: one FP32x2 multiply and four
-// integer maxima per pair of j).
+// (the largest single acc and jerk terms: one FP32x2 multiply and two
+// three-input integer maxima per pair of j).
 constexpr int kVarStats = 16;
 
 // Consume one shared-memory tile: this thread's j are kbase + m*JL.
@@ -544,8 +544,8 @@ __device__ __forceinline__ void to_partial(const StateMixedP &s, Partial &q) {
     q.pot = s.Pt;
     q.nn_r2 = (double)s.nr2;
     q.nn_j = s.nj;
-    q.qa = -2.f * __uint_as_float(max(s.qa0, s.qa1));  // max m / r^2
-    q.qj = __int_as_float(max(s.qj0, s.qj1));          // max m / r^3
+    q.qa = -2.f * __uint_as_float(s.qa);  // max m / r^2
+    q.qj = __int_as_float(s.qj);          // max m / r^3
 }
 __device__ __forceinline__ void to_partial(const StateF64 &s, Partial &q) {
     q.acc[0] = s.Ax; q.acc[1] = s.Ay; q.acc[2] = s.Az;
