@@ -423,9 +423,9 @@ __device__ __forceinline__ void fold(StateMixedBase &s) {
     s.ax = s.ay = s.az = s.jx = s.jy = s.jz = s.pt = 0.f;
 }
 
-// Variant bits of the mixed kernels: 2 = inner j-loop unrolled by 4 (else
-// 2).  Unrolling by 4 measured 1.3% faster for the scalar layout and equal
-// for the paired one.
+// Variant bits of the mixed kernels: 2 = inner j-loop of the scalar layout
+// unrolled by 4 (else 2): 1.3% faster.  (The paired layout's loop is
+// unrolled by 16 with the indicators on, by 4 otherwise.)
 constexpr int kVarUnroll4 = 2;
 // 4 = GRAPE-4 pipeline (FP64 kernel only; see the file header).
 constexpr int kVarG4 = 4;
@@ -465,14 +465,28 @@ __device__ __forceinline__ void consume_tile(typename StateOf<K>::type (&st)[R],
             }
             return;
         }
+        // The single-call kernels (error indicators on) unroll by 16
+        // (measured against 2, 4, 8 and 32 on the N = 262144 sweep: 97.6 ms
+        // at 4, 95.1 at 16; 32 spills); the batched and resident kernels,
+        // which hold three lane shapes in one body, by 4 (at 16 they spill).
         for (int m0 = 0; m0 < per; m0 += kFlushPairs) {
             const int m1 = min(m0 + kFlushPairs, per);
-#pragma unroll 4
-            for (int m = m0; m < m1; ++m) {
-                const int k = kbase + m * JL;
-                const JPairMixed J = S[k];
+            if constexpr (ST) {
+#pragma unroll 16
+                for (int m = m0; m < m1; ++m) {
+                    const int k = kbase + m * JL;
+                    const JPairMixed J = S[k];
 #pragma unroll
-                for (int r = 0; r < R; ++r) interact_pair<CHK, NB, IDENT, PO, ST>(st[r], J, tb + 2 * k, eps2, p);
+                    for (int r = 0; r < R; ++r) interact_pair<CHK, NB, IDENT, PO, ST>(st[r], J, tb + 2 * k, eps2, p);
+                }
+            } else {
+#pragma unroll 4
+                for (int m = m0; m < m1; ++m) {
+                    const int k = kbase + m * JL;
+                    const JPairMixed J = S[k];
+#pragma unroll
+                    for (int r = 0; r < R; ++r) interact_pair<CHK, NB, IDENT, PO, ST>(st[r], J, tb + 2 * k, eps2, p);
+                }
             }
 #pragma unroll
             for (int r = 0; r < R; ++r) fold_any<PO>(st[r]);
@@ -604,8 +618,12 @@ __device__ __forceinline__ Partial load_partial_cg(const Partial *src) {
     return a;
 }
 
+// MAPPED: honour p.out_map (only the FP64 layout's kernels, which run the
+// refinement's pass, and the generic reduction kernels compile it in: in
+// the paired mixed batch kernel it cost 100 bytes of spills).
+template <bool MAPPED = true>
 __device__ __forceinline__ void write_final(const ForceParams &p, int i, const Partial &q) {
-    const size_t o = p.out_map ? (size_t)p.out_map[i] : (size_t)i;
+    const size_t o = MAPPED && p.out_map ? (size_t)p.out_map[i] : (size_t)i;
 #pragma unroll
     for (int c = 0; c < 3; c++) {
         p.out_acc[3 * o + c] = q.acc[c];
@@ -756,7 +774,7 @@ __device__ __forceinline__ bool process_task(const ForceParams &p, int itile_idx
             const int i = i0 + r * IL;
             if (i >= p.ni) continue;
             if (p.nsplit == 1 && !p.keep_partials)
-                write_final(p, i, q[r]);
+                write_final<K == kKernF64>(p, i, q[r]);
             else
                 p.part[(size_t)split * p.ni + i] = q[r];
         }
@@ -786,7 +804,7 @@ __device__ __forceinline__ bool process_task(const ForceParams &p, int itile_idx
                     for (int u = 0; u < 4; ++u) add_partial(a, b[u]);
                 }
                 for (; sp < p.nsplit; ++sp) add_partial(a, load_partial_cg(p.part + (size_t)sp * p.ni + i));
-                write_final(p, i, a);
+                write_final<K == kKernF64>(p, i, a);
             }
             if (threadIdx.x == 0) p.tile_counter[itile_idx] = 0;
         }
