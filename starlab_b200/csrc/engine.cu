@@ -92,6 +92,7 @@ Engine::Engine(int cluster_id) : cluster_id_(cluster_id) {
     fault_pot_at_ = env_ll("G6B200_FAULT_POT", -1);
     small_enabled_ = env_int("G6B200_SMALL_CALLS", 1) != 0;
     refine_enabled_ = env_int("G6B200_REFINE", 1) != 0;
+    mixed_min_work_ = env_ll("G6B200_MIXED_MIN_WORK", 1LL << 25);
 }
 
 Engine::~Engine() { close(); }
@@ -185,7 +186,7 @@ void Engine::close() {
     stream_ = nullptr;
     cap_ = 0; call_cap_ = 0; part_cap_ = 0; nb_alloc_ = 0;
     n_staged_ = 0; slot_of_.clear(); nonident_.clear(); n_nonident_ = 0;
-    pred_valid_ = false; pending_ = false; xmax_ = 0; E_ = -1000;
+    pred_valid_ = pred64_valid_ = false; pending_ = false; xmax_ = 0; E_ = -1000;
     open_ = false;
 }
 
@@ -206,7 +207,7 @@ int Engine::reset() {
     for (int k = 0; k < n_staged_; ++k) slot_of_[h_stage_addr_[k]] = -1;
     n_staged_ = 0;
     pending_ = false;
-    pred_valid_ = false;
+    pred_valid_ = pred64_valid_ = false;
     last_error.clear();
     return 0;
 }
@@ -255,7 +256,7 @@ int Engine::ensure_capacity(int address) {
     cap_ = ncap;
     slot_of_.resize(cap_, -1);
     nonident_.resize(cap_, 0);
-    pred_valid_ = false;
+    pred_valid_ = pred64_valid_ = false;
     return 0;
 }
 
@@ -321,7 +322,7 @@ int Engine::flush_j() {
     stats_.h2d_bytes += (long long)n * (JF_COUNT * 8 + 8);
     for (int k = 0; k < n; ++k) slot_of_[h_stage_addr_[k]] = -1;
     n_staged_ = 0;
-    pred_valid_ = false;
+    pred_valid_ = pred64_valid_ = false;
     return 0;
 }
 
@@ -441,7 +442,7 @@ int Engine::set_j_bulk(int n, const int *address, const int *index, const double
             n_nonident_ += ni ? 1 : -1;
         }
     }
-    pred_valid_ = false;
+    pred_valid_ = pred64_valid_ = false;
     return 0;
 }
 
@@ -531,15 +532,7 @@ int Engine::ensure_refine_buffers(int ni) {
         ref_cap_ = n;
         stats_.grows++;
     }
-    if (jrec64_cap_ < cap_) {
-        if (d_jrec64_) cudaFree(d_jrec64_);
-        d_jrec64_ = nullptr;
-        jrec64_cap_ = 0;
-        G6_CHECK(cudaMalloc(&d_jrec64_, sizeof(JRecF64) * (size_t)cap_), "refine");
-        jrec64_cap_ = cap_;
-        pred64_valid_ = false;
-    }
-    return 0;
+    return ensure_jrec64();
 }
 
 int Engine::firsthalf(int nj, int ni, const int *index, const double (*xi)[3], const double (*vi)[3],
@@ -646,13 +639,50 @@ int Engine::firsthalf_impl(int nj, int ni, const int *index, const double (*xi)[
     return 0;
 }
 
+// Record that the j-records of layout km (the mixed ones in d_jrec_, or the
+// FP64 ones in d_jrec64_ when the engine is in mixed mode) hold the current
+// j-state at the block time.
+void Engine::mark_predicted(int nj, int km) {
+    if (mode_ == kModeMixed && km == kKernF64) {
+        pred64_valid_ = true;
+        pred64_ti_ = ti_;
+        pred64_nj_ = nj;
+        return;
+    }
+    pred_valid_ = true;
+    pred_ti_ = ti_;
+    pred_nj_ = nj;
+    pred_mode_ = km;
+    pred_E_ = E_;
+}
+
+// FP64 j-records beside the mixed ones (the refinement and the FP64 small
+// calls of the mixed mode), for the j-memory's capacity.
+int Engine::ensure_jrec64() {
+    if (jrec64_cap_ >= cap_) return 0;
+    if (d_jrec64_) cudaFree(d_jrec64_);
+    d_jrec64_ = nullptr;
+    jrec64_cap_ = 0;
+    G6_CHECK(cudaMalloc(&d_jrec64_, sizeof(JRecF64) * (size_t)cap_), "FP64 records");
+    jrec64_cap_ = cap_;
+    pred64_valid_ = false;
+    return 0;
+}
+
 int Engine::launch_call() {
     const int ni = call_ni_, nj = call_nj_;
     call_refine_ = false;
-    const int km = kmode();
+    // Mixed mode: a call of fewer than mixed_min_work_ interactions runs in
+    // FP64 on the FP64 j-records (d_jrec64_, kept beside the mixed ones):
+    // such calls are latency-bound, so FP64 costs them nothing, and they get
+    // FP64 results (kira's small blocks at its tiny first steps among them).
+    call_f64_ = mode_ == kModeMixed && mixed_min_work_ > 0 && !call_g4_ && !call_split_ && !call_sweep_ &&
+                !call_pot_ && !call_energy_ && (long long)ni * round_up(nj, tile_size(kmode())) < mixed_min_work_;
+    const int km = call_f64_ ? kKernF64 : kmode();
     const int T = tile_size(km);
     const int nj_pad = round_up(nj, T);
     if (nj_pad > cap_ && ensure_capacity(nj_pad - 1)) return -1;
+    if (call_f64_ && ensure_jrec64()) return -1;
     int E = std::max(E_, choose_E(xmax_));
     if (E != E_) {
         E_ = E;
@@ -674,9 +704,19 @@ int Engine::launch_call() {
     }
     unsigned *status = status2 + call_parity_;
     pred_timed_ = false;
-    const bool need_pred = !pred_valid_ || pred_ti_ != ti_ || pred_nj_ != nj || pred_mode_ != km || pred_E_ != E_ ||
-                           (small && n_staged_ > 0);
-    if (need_pred) pred64_valid_ = v2_valid_ = false;  // the refinement's FP64 records and |v| scale follow
+    const bool staged = small && n_staged_ > 0;
+    bool need_pred;
+    if (call_f64_) {
+        need_pred = !pred64_valid_ || pred64_ti_ != ti_ || pred64_nj_ != nj || staged;
+        if (staged) pred_valid_ = v2_valid_ = false;  // the updates land in the raw j-state: the mixed records are stale
+    } else {
+        need_pred = !pred_valid_ || pred_ti_ != ti_ || pred_nj_ != nj || pred_mode_ != km || pred_E_ != E_ || staged;
+        if (need_pred) pred64_valid_ = v2_valid_ = false;  // the FP64 records and |v| scale follow
+    }
+    void *jrec = call_f64_ ? d_jrec64_ : d_jrec_;
+    // FP64 records are predicted over the mixed layout's padding too (the
+    // refinement reads them with the same nj).
+    const int pred_pad = call_f64_ ? round_up(nj, tile_size(kmode())) : nj_pad;
     if (small) {
         // Updates, prediction and i-records in one launch whose parameter is
         // the call's host data (no host->device copy).
@@ -684,7 +724,7 @@ int Engine::launch_call() {
         sc.n_upd = n_staged_;
         sc.ni = ni;
         sc.nj = nj;
-        sc.nj_pad = nj_pad;
+        sc.nj_pad = pred_pad;
         sc.cap = cap_;
         sc.predict = need_pred;
         sc.parity = call_parity_;
@@ -706,32 +746,24 @@ int Engine::launch_call() {
         stats_.h2d_bytes += (long long)sizeof(SmallCall);
         n_staged_ = 0;
         if (timed_) G6_CHECK(cudaEventRecord(ev_pred0_, stream_), "event");
-        launch_small_call(stream_, km, sc, d_jraw_, d_jindex_, d_jrec_, d_irec_, d_ieps2_, status2);
+        launch_small_call(stream_, km, sc, d_jraw_, d_jindex_, jrec, d_irec_, d_ieps2_, status2);
         G6_CHECK(cudaGetLastError(), "small call launch");
         stats_.launches++;
         if (timed_) G6_CHECK(cudaEventRecord(ev_pred1_, stream_), "event");
         pred_timed_ = need_pred;
         if (need_pred) {
             stats_.predictions++;
-            pred_valid_ = true;
-            pred_ti_ = ti_;
-            pred_nj_ = nj;
-            pred_mode_ = km;
-            pred_E_ = E_;
+            mark_predicted(nj, km);
         }
     } else if (need_pred) {
         if (timed_) G6_CHECK(cudaEventRecord(ev_pred0_, stream_), "event");
-        launch_predict(stream_, km, d_jraw_, d_jindex_, cap_, nj, nj_pad, ti_, fs, d_jrec_, status);
+        launch_predict(stream_, km, d_jraw_, d_jindex_, cap_, nj, pred_pad, ti_, fs, jrec, status);
         G6_CHECK(cudaGetLastError(), "predict launch");
         stats_.launches++;
         if (timed_) G6_CHECK(cudaEventRecord(ev_pred1_, stream_), "event");
         stats_.predictions++;
         pred_timed_ = true;
-        pred_valid_ = true;
-        pred_ti_ = ti_;
-        pred_nj_ = nj;
-        pred_mode_ = km;
-        pred_E_ = E_;
+        mark_predicted(nj, km);
     }
     if (ni > 0) {
         if (small) {
@@ -766,7 +798,7 @@ int Engine::launch_call() {
             return -1;
         last_cfg_ = cfg;
         ForceParams p{};
-        p.jrec = d_jrec_;
+        p.jrec = jrec;
         p.nj = nj;
         p.nj_pad = nj_pad;
         p.irec = d_irec_;
@@ -800,11 +832,11 @@ int Engine::launch_call() {
                 stats_.launches += 2;
                 v2_valid_ = true;
             }
-            if (!pred64_valid_) {
+            if (!pred64_valid_ || pred64_ti_ != ti_ || pred64_nj_ != nj) {
                 launch_predict(stream_, kKernF64, d_jraw_, d_jindex_, cap_, nj, nj_pad, ti_, fs, d_jrec64_, status);
                 G6_CHECK(cudaGetLastError(), "refine predict launch");
                 stats_.launches++;
-                pred64_valid_ = true;
+                mark_predicted(nj, kKernF64);
             }
             RefineArgs ra{};
             ra.ni = ni;

@@ -225,6 +225,10 @@ class Engine {
     // the host data as its parameter (G6B200_SMALL_CALLS=0 turns it off).
     bool small_enabled_ = true;
     bool refine_enabled_ = true;  // G6B200_REFINE=0: mixed mode without the FP64 recomputation
+    long long mixed_min_work_ = 1LL << 25;  // mixed mode: calls of fewer interactions run in FP64
+    bool call_f64_ = false;                 // this call runs on the FP64 records
+    void mark_predicted(int nj, int km);
+    int ensure_jrec64();
     bool call_small_ = false;
     int small_parity_ = 0;  // status word the next small call reports into
     int call_parity_ = 0;   // status word of the call in flight

@@ -27,7 +27,10 @@ def _engine(mode, cid, npipes=8192):
 
 
 @pytest.mark.parametrize("mode", ["fp64", "mixed"])
-def test_potential_only_matches_oracle_and_full_kernel(mode, oracle):
+def test_potential_only_matches_oracle_and_full_kernel(mode, oracle, monkeypatch):
+    # the mixed mode's full calls below 2^25 interactions run in FP64;
+    # here every full call stays mixed, to compare the two mixed kernels
+    monkeypatch.setenv("G6B200_MIXED_MIN_WORK", "0")
     n = 8192
     m, x, v, a, j = snapshot(n, 41)
     ti = 1.0 / 128

@@ -214,10 +214,12 @@ def test_unsoftened_and_repeated_updates(oracle):
     eng.close()
 
 
-def test_fixed_point_range_widening(oracle):
+def test_fixed_point_range_widening(oracle, monkeypatch):
     """A particle far outside the initial range: the engine widens the
-    fixed-point range and recomputes; results stay within tolerance."""
+    fixed-point range and recomputes; results stay within tolerance.  (The
+    calls are small: the mixed path is forced, G6B200_MIXED_MIN_WORK=0.)"""
     from starlab_b200 import ics
+    monkeypatch.setenv("G6B200_MIXED_MIN_WORK", "0")
     n = 2048
     m, x, v = ics.plummer(n, 3)
     z = np.zeros((n, 3))
@@ -343,3 +345,56 @@ def test_mixed_every_particle_within_tolerance(case, oracle):
     samp = np.linspace(0, len(m) - 1, 64).astype(np.int32)
     ra, rj, rp, _, _ = oracle.force(xp, vp, m, samp, xp[samp], vp[samp], eps2)
     assert rel_err_vec(ref[0][samp], ra).max() < 1e-12 and rel_err(ref[2][samp], rp).max() < 1e-12
+
+
+def test_mixed_mode_small_calls_run_fp64(c2, monkeypatch):
+    """Mixed mode runs a call of fewer than G6B200_MIXED_MIN_WORK (2^25)
+    interactions on FP64 j-records kept beside the mixed ones: its results
+    are bit-identical to the FP64 engine's, through the copy path and the
+    one-launch path with staged updates, interleaved with large (mixed)
+    calls at the same and at a new block time.  With the threshold at 0 the
+    same small call runs in mixed precision."""
+    n = c2["n"]
+    rng = np.random.default_rng(9)
+    emx, e64 = new_engine("mixed"), new_engine("fp64")
+    for e in (emx, e64):
+        load(e, c2)
+        e.set_ti(TI)
+    idx = np.arange(n, dtype=np.int32)
+
+    def both(s, ni):
+        sl = slice(s, s + ni)
+        return [e.force(n, idx[sl], c2["xp"][sl], c2["vp"][sl], EPS2) for e in (emx, e64)]
+
+    def same(a, b):
+        for u, w in zip(a, b):
+            assert np.array_equal(u, w)
+
+    same(*both(100, 16))                      # small: FP64 records, copy path
+    big_mx, big_64 = both(0, 4096)            # 4096 x 65536 > 2^25: mixed
+    assert rel_err_vec(big_mx[0], big_64[0]).max() <= 1e-6 and not np.array_equal(big_mx[0], big_64[0])
+    same(*both(7, 200))                       # small again at the same block time
+    for e in (emx, e64):                      # staged updates: the one-launch path
+        for k in (3, 50, 4000):
+            e.set_j_particle(k, 0.0, c2["m"][k] * 1.01, np.zeros(3), c2["j"][k] / 6.0, 0.5 * c2["a"][k],
+                             c2["v"][k], c2["x"][k] + 1e-4)
+    same(*both(40, 32))
+    for e in (emx, e64):
+        e.set_ti(TI * 1.5)
+    same(*both(5000, 64))
+    big_mx, big_64 = both(1000, 4096)
+    assert rel_err_vec(big_mx[0], big_64[0]).max() <= 1e-6
+    same(*both(0, 1))
+    emx.close()
+    monkeypatch.setenv("G6B200_MIXED_MIN_WORK", "0")
+    e0 = new_engine("mixed")
+    load(e0, c2)
+    e0.set_ti(TI)
+    a0 = e0.force(n, idx[100:116], c2["xp"][100:116], c2["vp"][100:116], EPS2)
+    e64_fresh = new_engine("fp64")
+    load(e64_fresh, c2)
+    e64_fresh.set_ti(TI)
+    r0 = e64_fresh.force(n, idx[100:116], c2["xp"][100:116], c2["vp"][100:116], EPS2)
+    assert not np.array_equal(a0[0], r0[0]) and rel_err_vec(a0[0], r0[0]).max() <= 1e-6
+    for e in (e0, e64, e64_fresh):
+        e.close()
