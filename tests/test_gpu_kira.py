@@ -159,3 +159,28 @@ def test_kira_jp_buffer_mode_identical(plummer1024):
     ep, ed = energies(plain), energies(dma)
     assert len(ep) >= 4 and ep == ed, (ep, ed)
 
+
+
+def test_kira_mixed_step_count_near_fp64(tmp_path):
+    """kira in the mixed mode takes the FP64 run's steps, near enough: N =
+    32768 Plummer (seed 42), calls of up to 4096 i (G6B200_NPIPES) so the
+    large blocks run in mixed precision while blocks below 2^25
+    interactions run in FP64, t = 1/32.  The force-call count stays within
+    1.2x of the FP64 run's (with every call mixed it was 25x at N = 8192),
+    and the mixed run did use the mixed kernels (particles refined)."""
+    mk = _need("makeplummer")
+    snap = os.path.join(tmp_path, "p32k.snap")
+    with open(snap, "w") as f:
+        subprocess.run([mk, "-n", "32768", "-s", "42", "-i"], stdout=f, stderr=subprocess.DEVNULL, check=True)
+    args = ["-t", "0.03125", "-d", "0.015625", "-e", "0.001", "-a", "0.02"]
+    runs = {}
+    for prec in ("fp64", "mixed"):
+        log = run_kira(_need("kira_g6"), snap, args,
+                       {"G6B200_PRECISION": prec, "G6B200_NPIPES": "4096", "G6B200_TRACE": "1"}, str(tmp_path))
+        runs[prec] = (_trace(log, "calls"), _trace(log, "refined"), energies(log))
+    (c64, _, e64), (cmx, refined, emx) = runs["fp64"], runs["mixed"]
+    print("kira N=32768: calls fp64 %d mixed %d, refined %d, dE fp64 %.2e mixed %.2e"
+          % (c64, cmx, refined, abs(e64[-1] - e64[0]), abs(emx[-1] - emx[0])))
+    assert cmx <= 1.2 * c64, (cmx, c64)
+    assert refined > 0
+    assert abs(emx[-1] - emx[0]) <= 1e-8 * abs(emx[0])
