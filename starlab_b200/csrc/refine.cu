@@ -10,12 +10,13 @@
 // engine, every particle whose acc error exceeds 0.4e-6 has qa/|a| >= 1.2
 // and every one whose jerk error exceeds 4e-6 has qj v_rms/|jerk| >= 2.0
 // (v_rms: rms speed of the j-set).  A particle is flagged when qa/|a| >
-// kRefineA or qj v_rms/|jerk| > kRefineJ (1-2% of a Plummer sphere) and
+// kRefineA or qj v_rms/|jerk| > kRefineJ (about 2% of a Plummer sphere) and
 // recomputed with the FP64 kernel against FP64 j-records of the same block
 // time; its results replace the mixed ones.
-// Everything stays on the device: flagging and compaction, the item of the
-// FP64 pass (its size read on the device by the batched kernel), the
-// scatter of the results.
+// Everything stays on the device, in two launches: flagging and compaction
+// (the flag kernel's last block builds the FP64 pass's work item, its size
+// read on the device by the batched kernel), and the FP64 pass, which
+// writes the flagged particles' rows of the call's outputs (out_map).
 #include <cmath>
 #include "common.cuh"
 #include "kernels.h"
