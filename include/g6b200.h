@@ -35,7 +35,9 @@
  *                      conditioned (large, nearly cancelling terms: error
  *                      indicators accumulated by the kernel) recomputed in
  *                      FP64, so every particle meets acc, pot <= 1e-6 and
- *                      jerk <= 1e-5 relative to FP64.
+ *                      jerk <= 1e-5 relative to FP64.  Calls of fewer than
+ *                      G6B200_MIXED_MIN_WORK (2^25) interactions run in
+ *                      FP64 (they are latency-bound; kira's small blocks).
  */
 #ifndef G6B200_H
 #define G6B200_H
