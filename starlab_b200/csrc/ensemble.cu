@@ -622,6 +622,7 @@ class Ensemble {
     long long max_iters_ = 2000000;  // run guards (G6B200_ENS_MAX_ITERS / _SECONDS)
     double max_seconds_ = 600.0;
     bool fuse_ = true;  // G6B200_ENS_FUSED=0: every block step through the schedule kernel
+    int min_tiles_ = 4;  // G6B200_ENS_MIN_TILES: fewest j-tiles per task (1, 2, 4 or 8)
     std::vector<int> off_;
     std::vector<double> hm_, hx_, hv_;  // host copies of the initial state
     EnsDev d_{};
@@ -654,6 +655,10 @@ int Ensemble::setup() {
     if (const char *e = getenv("G6B200_ENS_MAX_ITERS")) max_iters_ = atoll(e);
     if (const char *e = getenv("G6B200_ENS_MAX_SECONDS")) max_seconds_ = atof(e);
     if (const char *e = getenv("G6B200_ENS_FUSED")) fuse_ = atoi(e) != 0;
+    if (const char *e = getenv("G6B200_ENS_MIN_TILES")) {
+        const int v = atoi(e);
+        min_tiles_ = v <= 1 ? 1 : (v <= 2 ? 2 : (v <= 4 ? 4 : 8));
+    }
     ECHK(cudaSetDevice(device_), "device");
     ECHK(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "stream");
     ECHK(cudaDeviceGetAttribute(&num_sms_, cudaDevAttrMultiProcessorCount, device_), "attr");
@@ -668,7 +673,7 @@ int Ensemble::setup() {
         for (int g = off_[c]; g < off_[c + 1]; ++g) cid[g] = c;
         poff[c] = ptot;
         const int nj_pad = (n_[c] + tile_of(kmode_) - 1) / tile_of(kmode_) * tile_of(kmode_);
-        ptot += (long long)n_[c] * batch_max_split(kmode_, nj_pad);
+        ptot += (long long)n_[c] * batch_max_split(kmode_, nj_pad, min_tiles_);
     }
     auto alloc = [&](void **p, size_t bytes) -> cudaError_t {
         cudaError_t e = cudaMalloc(p, bytes > 0 ? bytes : 16);
@@ -727,6 +732,7 @@ int Ensemble::setup() {
     // servers' work cap instead the bench's ensemble ran 249-270 us per
     // iteration against 225.
     d_.cfg.nsplit = 592;
+    d_.cfg.min_tiles = min_tiles_;
     ctas_ = batch_ctas(kmode_, d_.cfg, num_sms_);
     ECHK(cudaMemcpyAsync((void *)d_.off, off_.data(), sizeof(int) * (nc_ + 1), cudaMemcpyHostToDevice, stream_), "copy");
     ECHK(cudaMemcpyAsync((void *)d_.n, n_.data(), sizeof(int) * nc_, cudaMemcpyHostToDevice, stream_), "copy");

@@ -99,6 +99,7 @@ struct ForceConfig {
     int H;        // j-subranges per CTA
     int nsplit;   // CTAs along j
     int jper = 0; // > 0: j per split fixed (a multiple of the tile); nsplit follows
+    int min_tiles = 4;  // batched plans: fewest j-tiles per split (1, 2, 4 or 8)
 };
 
 void launch_scatter(cudaStream_t s, int n, const int *addr, const int *index, const double *vals,
@@ -194,7 +195,8 @@ __host__ __device__ inline int batch_item_itile(int kmode, const ForceConfig &cf
 // by the ensemble's tuner; else 592 = 4 x 148 but no more than one task per
 // kMinTaskWork interactions (the servers: small calls stay in few tasks, so
 // a batch of many calls is not cut into tasks too small to keep the
-// pipeline busy); at least 4 tiles per split.
+// pipeline busy); at least cfg.min_tiles tiles per split (4 unless the
+// ensemble asks for shorter tasks).
 constexpr long long kMinTaskWork = 65536;
 __host__ __device__ inline void batch_plan(int kmode, const ForceConfig &cfg, ForceParams &item, int &n_tasks) {
     const long long work_cap = ((long long)item.ni * item.nj_pad) / kMinTaskWork;
@@ -216,7 +218,8 @@ __host__ __device__ inline void batch_plan(int kmode, const ForceConfig &cfg, Fo
         item.jper = T;
     } else {
         int sp = (kTargetTasks + n_itiles - 1) / n_itiles;
-        const int cap = (ntiles + 3) / 4;
+        const int mt = cfg.min_tiles > 1 ? cfg.min_tiles : 1;
+        const int cap = (ntiles + mt - 1) / mt;
         sp = sp < cap ? sp : cap;
         sp = sp > 1 ? sp : 1;
         const int per_split_tiles = (ntiles + sp - 1) / sp;
@@ -226,10 +229,12 @@ __host__ __device__ inline void batch_plan(int kmode, const ForceConfig &cfg, Fo
     n_tasks = n_itiles * item.nsplit;
 }
 
-// Largest nsplit batch_plan can choose for nj_pad (sizes the partials).
-__host__ __device__ inline int batch_max_split(int kmode, int nj_pad) {
+// Largest nsplit batch_plan can choose for nj_pad with at least min_tiles
+// tiles per split (sizes the partials).
+__host__ __device__ inline int batch_max_split(int kmode, int nj_pad, int min_tiles = 4) {
     const int ntiles = nj_pad / tile_of(kmode);
-    const int cap = (ntiles + 3) / 4;
+    const int mt = min_tiles > 1 ? min_tiles : 1;
+    const int cap = (ntiles + mt - 1) / mt;
     return cap > 1 ? cap : 1;
 }
 ForceConfig batch_config(int kmode);
