@@ -286,7 +286,20 @@ struct RefineArgs {
 };
 void launch_refine_v2(cudaStream_t s, const double *jraw, int cap, int nj, double *work);
 cudaError_t launch_refine(cudaStream_t s, const RefineArgs &r, int num_sms);
-size_t refine_partial_records(int ni);
+// Tasks wanted by the refinement's FP64 pass over `count` flagged i against
+// nj_pad j: one per kMinTaskWork interactions (as the servers' plan), but no
+// fewer than kRefineMinTasks -- a call with a handful of flagged particles
+// otherwise ran as a dozen CTAs walking long j-ranges (ni = 128: 0.32 ms
+// with the refinement vs 0.12 ms without) -- and no more than 592.
+constexpr int kRefineMinTasks = 128;
+__host__ __device__ inline int refine_tasks_wanted(int count, int nj_pad) {
+    const long long wc = (long long)count * nj_pad / kMinTaskWork;
+    return (int)(wc < kRefineMinTasks ? kRefineMinTasks : (wc > 592 ? 592 : wc));
+}
+// Split partial records the FP64 pass of a call of ni i can use: at most
+// 592 tasks over i-tiles of at most 64 i, so nsplit x flagged stays below
+// 592 x 64 + flagged.
+__host__ __device__ inline size_t refine_partial_records(int ni) { return 64 * 600 + (size_t)ni; }
 
 // Neighbour lists: per-i sort + compaction into ascending address order.
 // offsets[ni+1] (exclusive scan of min(count, cap)), out[total].

@@ -61,19 +61,14 @@ __global__ void __launch_bounds__(kThreads) v2_total_kernel(double *work, int nj
     if (threadIdx.x == 0) work[kRefineBlocks] = nj > 0 ? s / nj : 0.0;  // mean |v|^2
 }
 
-// One FP64 work item for the flagged particles, sized by their count.
-// Tasks wanted: one per kMinTaskWork interactions (as the servers' plan),
-// but no fewer than kRefineMinTasks -- a call with a handful of flagged
-// particles otherwise ran as a dozen CTAs walking long j-ranges (ni = 128:
-// 0.32 ms with the refinement vs 0.12 ms without) -- and no more than 592.
-// The item writes its results straight into the flagged particles' rows of
-// the call's outputs (out_map = the flag list).
-constexpr int kRefineMinTasks = 128;
+// One FP64 work item for the flagged particles, sized by their count
+// (tasks wanted: refine_tasks_wanted).  The item writes its results straight
+// into the flagged particles' rows of the call's outputs (out_map = the
+// flag list).
 __device__ void make_refine_item(ForceParams p, ForceConfig cfg, int count, ForceParams *items, int *pre,
                                  int *counter) {
     p.ni = count;
-    const long long wc = (long long)p.ni * p.nj_pad / kMinTaskWork;
-    cfg.nsplit = (int)(wc < kRefineMinTasks ? kRefineMinTasks : (wc > 592 ? 592 : wc));
+    cfg.nsplit = refine_tasks_wanted(p.ni, p.nj_pad);
     int nt = 0;
     batch_plan(kKernF64, cfg, p, nt);
     items[0] = p;
@@ -162,7 +157,5 @@ cudaError_t launch_refine(cudaStream_t s, const RefineArgs &r, int num_sms) {
     if (e != cudaSuccess) return e;
     return cudaGetLastError();
 }
-
-size_t refine_partial_records(int ni) { return 64 * 600 + (size_t)ni; }
 
 }  // namespace g6

@@ -11,6 +11,9 @@
 //   jper a positive multiple of the tile; every split non-empty; the splits
 //   cover all nj_pad j; nsplit <= batch_max_split; n_tasks = i-tiles x
 //   nsplit with the i-tiles covering ni; H a power of two dividing the warps.
+// The mixed mode's FP64 refinement pass (refine.cu) plans its flagged
+// particles the same way with refine_tasks_wanted; its partials buffer holds
+// refine_partial_records(ni) records, checked against nsplit x flagged.
 // Prints "ok <plans checked>" or the first violation, and exits 1 on one.
 #include <cstdio>
 #include <vector>
@@ -82,6 +85,25 @@ int main() {
                         }
                     }
                 }
+    }
+    // the refinement's FP64 pass: `count` flagged i of a call, any j-count
+    for (int nj : sizes) {
+        const int nj_pad = (nj + tile_of(kKernF64) - 1) / tile_of(kKernF64) * tile_of(kKernF64);
+        for (int count : sizes) {
+            ForceConfig c = base_config();
+            c.nsplit = refine_tasks_wanted(count, nj_pad);
+            ForceParams p{};
+            p.ni = count;
+            p.nj = nj;
+            p.nj_pad = nj_pad;
+            int nt = -1;
+            batch_plan(kKernF64, c, p, nt);
+            ++checked;
+            if ((size_t)p.nsplit * (size_t)count > refine_partial_records(count))
+                return fail("refinement partials above refine_partial_records", kKernF64, c, count, nj_pad, p);
+            if ((long long)p.nsplit * p.jper < nj_pad || (long long)(p.nsplit - 1) * p.jper >= nj_pad)
+                return fail("refinement splits do not tile the j-set", kKernF64, c, count, nj_pad, p);
+        }
     }
     std::printf("ok %lld\n", checked);
     return 0;
