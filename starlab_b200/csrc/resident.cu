@@ -580,7 +580,9 @@ class Resident {
         bool held = false;
     };
     int launch_locked();
+    int launch_try_locked(bool &kernel_died);
     void recover_locked();
+    void fail_slots_locked(int state);
     static FixedScale scale_of(int E) {
         FixedScale fs;
         fs.to_units = std::ldexp(1.0, 23 - E);
@@ -910,7 +912,7 @@ long long Resident::submit(int c, double ti, int nj, int ni, const int *index, c
     }
     h.held = false;
     __atomic_store_n(&s.state, (int)kReady, __ATOMIC_RELEASE);
-    if (launch_locked()) return -1;
+    launch_locked();  // when it fails, the call is marked failed and its wait reports it
     return id;
 }
 
@@ -931,14 +933,37 @@ void Resident::hold(bool on) {
 }
 
 // Kernel not running (it left after its idle time, or after an error) and a
-// call waiting: launch it again.  Called with mu_ held.
+// call waiting: launch it again.  Called with mu_ held.  When that fails,
+// the calls no kernel will serve -- the READY ones, and the TAKEN ones too
+// when the previous kernel died with a CUDA error -- are marked failed, so
+// their waiters return and free their slots.
 int Resident::launch_locked() {
+    bool kernel_died = false;
+    const int rc = launch_try_locked(kernel_died);
+    if (rc) {
+        if (kernel_died) fail_slots_locked(kTaken);
+        fail_slots_locked(kReady);
+        cv_idle_.notify_all();
+    }
+    return rc;
+}
+
+void Resident::fail_slots_locked(int state) {
+    for (int k = 0; k < kResSlots; ++k)
+        if (__atomic_load_n(&slots_[k].state, __ATOMIC_ACQUIRE) == state) {
+            slots_[k].status |= kLostWithKernel;
+            __atomic_store_n(&slots_[k].state, (int)kFailed, __ATOMIC_RELEASE);
+        }
+}
+
+int Resident::launch_try_locked(bool &kernel_died) {
     if (launched_) {
         const cudaError_t q = cudaEventQuery(ev_run_);
         if (q == cudaErrorNotReady) return 0;  // running
         launched_ = false;
         if (q != cudaSuccess) {
             err = std::string("resident: kernel failed: ") + cudaGetErrorString(q);
+            kernel_died = true;
             return -1;
         }
         if (__atomic_load_n(&ctl_->error, __ATOMIC_ACQUIRE)) recover_locked();
@@ -959,9 +984,17 @@ int Resident::launch_locked() {
         err = std::string("resident: launch failed: ") + cudaGetErrorString(e);
         return -1;
     }
-    RES_CHECK(cudaEventRecord(ev_run_, stream_), "launch");
-    launched_ = true;
     stats_.launches++;
+    const cudaError_t r = cudaEventRecord(ev_run_, stream_);
+    if (r != cudaSuccess) {
+        // The kernel runs but cannot be watched: wait for it to leave (it
+        // serves the READY calls, then exits after its idle time), so that no
+        // second kernel is launched beside it.
+        err = std::string("resident: launch: ") + cudaGetErrorString(r);
+        cudaStreamSynchronize(stream_);
+        return 0;
+    }
+    launched_ = true;
     return 0;
 }
 
@@ -970,11 +1003,7 @@ int Resident::launch_locked() {
 // i-tile arrival counters a cut-short batch may have left raised.
 void Resident::recover_locked() {
     __atomic_store_n(&ctl_->error, 0u, __ATOMIC_RELEASE);
-    for (int k = 0; k < kResSlots; ++k)
-        if (__atomic_load_n(&slots_[k].state, __ATOMIC_ACQUIRE) == kTaken) {
-            slots_[k].status |= kLostWithKernel;
-            __atomic_store_n(&slots_[k].state, (int)kFailed, __ATOMIC_RELEASE);
-        }
+    fail_slots_locked(kTaken);
     cudaMemsetAsync(dev_.tcnt, 0, 4 * dev_.i_cap, stream_);
     stats_.recoveries++;
 }
@@ -998,7 +1027,7 @@ int Resident::wait(long long id, double (*acc)[3], double (*jerk)[3], double *po
         if (st == kDone || st == kFailed) break;
         if ((spin & 1023) == 1023) {
             std::lock_guard<std::mutex> lk(mu_);
-            if (!h.held && launch_locked()) return -3;
+            if (!h.held) launch_locked();  // a failed launch fails this call: the loop then ends
             if (now_s() - t0 > 600.0) {
                 err = "resident: call not served within 600 s";
                 return -3;
