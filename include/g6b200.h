@@ -363,7 +363,8 @@ int g6b200_set_position_range(int cluster_id, double xmax);
  * of the cluster is in flight and copies the touched j rows with the copy
  * engine.  A call sees the j-particles set before it was submitted; its
  * results are bit-identical alone and in any mix.  wait returns 0, 2 (the
- * kernel left before the call completed), 3 (a j-tile copy wait timed out),
+ * kernel left before the call completed, or could not be launched for it),
+ * 3 (a j-tile copy wait timed out),
  * 4 (positions outside the fixed-point range: the range is widened, submit
  * again), < 0 (bad request).  hold(1) keeps calls from the kernel until
  * hold(0) releases them together.  selftest_stall makes the kernel's CTA 0
