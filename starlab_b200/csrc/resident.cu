@@ -846,8 +846,8 @@ long long Resident::submit(int c, double ti, int nj, int ni, const int *index, c
                            const double (*vi)[3]) {
     std::unique_lock<std::mutex> lk(mu_);
     auto it = clusters_.find(c);
-    if (it == clusters_.end() || ni < 0 || nj <= 0 || !started_) {
-        err = "resident: bad cluster or sizes";
+    if (it == clusters_.end() || ni < 0 || nj <= 0 || !started_ || (ni > 0 && (!index || !xi || !vi))) {
+        err = "resident: bad cluster, sizes or arrays";
         return -1;
     }
     Cluster &cl = *it->second;

@@ -320,6 +320,7 @@ int Server::set_j(int c, int n, const int *address, const double *tj, const doub
 
 long long Server::submit(int c, double ti, int nj, int ni, const int *index, const double (*xi)[3],
                          const double (*vi)[3]) {
+    if (ni < 0 || nj <= 0 || (ni > 0 && (!index || !xi || !vi))) return -1;  // before copying the arrays
     auto r = std::make_shared<Request>();
     r->cluster = c;
     r->ti = ti;
