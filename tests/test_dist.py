@@ -103,13 +103,13 @@ def _run_split(world):
 
 def test_split_cluster_bit_identical_across_world_sizes():
     """The j-split exchange (block partials -> MAX of exponents and r^2 ->
-    fixed-point SUM and j MAX -> FP64) gives the same bits on 1, 2 and 3
+    fixed-point SUM and j MAX -> FP64) gives the same bits on 1, 2, 3 and 4
     ranks (four blocks of 256 j dealt out contiguously), and the oracle's
     single-process answer within FP64 rounding (CPU stand-in for each
     rank's kernels: tests/split_cpu.py)."""
     import numpy as np
     from oracle.oracle import G6Oracle
-    runs = {w: _run_split(w) for w in (1, 2, 3)}
+    runs = {w: _run_split(w) for w in (1, 2, 3, 4)}
     base = runs[1][0]
     for w, out in runs.items():
         spans = [(o[5], o[6]) for o in out]
